@@ -1,0 +1,447 @@
+"""Benchmark: one full iteration (forward + volume VJP + per-view pose VJP) of the FP32
+projector on the full-scan workload, printed as one JSON line.
+
+Workload (one step): 256^3 FP32 chest-like phantom at 0.8 mm (seeded, synthetic), 360
+cone-beam views over 360 deg (SID 1000 mm, SDD 1500 mm), 512x512 detector at 0.8 mm,
+1024 clipped midpoint samples per ray; L2 loss against a seeded target image, its
+gradient with respect to the field and to a per-view 6-DoF pose tangent.
+
+Metric: realised ray-samples per second of the full iteration (a realised ray-sample
+is one midpoint sample on a ray whose clipped span is non-empty; S per such ray).
+``value`` is timed on the device with the inputs resident; ``e2e`` includes the
+host->device upload of field, target and pose tangent from pinned memory and the
+device->host read of loss, image and gradients every step.  Between timed steps the
+L2 cache is flushed by writing a 256 MiB buffer.
+
+``--impl reference`` times the CPU restatement of the reference projector (the oracle,
+all host threads) on a bounded sample of the same workload and prints the same line
+with ``"impl": "reference"``.
+
+Multi-GPU (torchrun, one rank per GPU): every rank projects its own 360 views (the views
+of an N x 360-view acquisition, sharded by view) and the volume gradient is summed over
+ranks with an NCCL all-reduce; ``value`` is the realised samples of all ranks divided
+by the slowest rank's time (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "ray-samples/s fwd+vol+pose VJP vs plain FP32; served p50/p99 at FP64 err≤1e-4"
+UNIT = "ray-samples/s"
+WORKLOAD = "fullscan 256^3 chest 0.8mm, 360 cone views SID1000/SDD1500, 512x512 @0.8mm, S=1024, L2 loss"
+
+
+def parse() -> argparse.Namespace:
+    parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=("dpt_b200", "reference"), default="dpt_b200")
+    parser.add_argument("--views", type=int, default=360, help="views per rank")
+    parser.add_argument("--size", type=int, default=256, help="grid samples per axis")
+    parser.add_argument("--detector", type=int, default=512)
+    parser.add_argument("--samples", type=int, default=1024)
+    parser.add_argument("--storage", choices=("float32", "bfloat16", "float16"), default="float32")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--seed", type=int, default=20261203)
+    return parser.parse_args()
+
+
+def rank_info() -> tuple[int, int, int]:
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.process = None
+
+    def start(self) -> None:
+        try:
+            self.process = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.process = None
+
+    def stop(self) -> dict | None:
+        if self.process is None:
+            return None
+        self.process.terminate()
+        try:
+            self.process.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.process.kill()
+        self.file.flush()
+        rows = [line.split(", ") for line in Path(self.file.name).read_text().splitlines() if line.strip()]
+        os.unlink(self.file.name)
+        samples = []
+        reasons: set[str] = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for row in rows:
+            try:
+                sm, sm_max = float(row[1]), float(row[2])
+            except (ValueError, IndexError):
+                continue
+            samples.append((sm, sm_max, float(row[3]) if row[3] not in ("[N/A]", "") else 0.0))
+            for name, flag in zip(names, row[5:9], strict=False):
+                if flag.strip().lower() == "active":
+                    reasons.add(name)
+        if not samples:
+            return None
+        loaded = [s for s in samples if s[2] > 300.0] or samples
+        return {"sm_mhz": statistics.median(s[0] for s in loaded), "sm_max_mhz": max(s[1] for s in samples),
+                "power_w_max": max(s[2] for s in samples), "samples": len(samples),
+                "reasons": sorted(reasons)}
+
+
+def build_workload(args, device):
+    """Grid, geometry, phantom, target pose tangent and seeded target image (untimed)."""
+    import numpy as np
+    import torch
+
+    from dpt_b200.geometry import ConeBeamIntrinsics
+    from dpt_b200.phantoms import centred_grid, chest_phantom
+
+    spacing = 0.8 * 256.0 / args.size
+    grid = centred_grid((args.size,) * 3, (spacing,) * 3)
+    intrinsics = ConeBeamIntrinsics(1000.0, 1500.0, (args.detector, args.detector),
+                                    (0.8 * 512.0 / args.detector,) * 2)
+    rank, world, _ = rank_info()
+    total_views = args.views * world
+    angles = tuple(2.0 * math.pi * (rank * args.views + k) / total_views for k in range(args.views))
+    geometry = intrinsics.batch(angles)
+    values = chest_phantom(grid, seed=args.seed)
+    rng = np.random.default_rng(args.seed + 1)
+    truth = rng.normal(size=(args.views, 6)) * np.array([0.5, 0.5, 0.5, 0.004, 0.004, 0.004])
+    return grid, geometry, values, torch.tensor(truth, dtype=torch.float64, device=device)
+
+
+# ------------------------------------------------------------------ helpers
+
+def measured_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic() -> dict | None:
+    """DRAM bytes per realised sample of the dominant kernel, from the committed ncu summary."""
+    path = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(path.read_text())
+    except (OSError, ValueError):
+        return None
+
+
+def algorithmic_bytes(kernel: str, storage_bytes: int) -> int:
+    """Bytes per realised ray-sample: forward 8 b_s; joint volume+pose VJP 8 b_s + 32."""
+    if kernel == "forward":
+        return 8 * storage_bytes
+    if kernel == "vjp":
+        return 8 * storage_bytes + 32
+    return 0
+
+
+def oracle_sample_rate(grid, geometry, values, samples: int, budget_s: float, threads: int,
+                       view: int = 0, storage: str = "float32"):
+    """Time the CPU oracle (forward + joint volume/pose VJP) on a block of detector rows of
+    one view sized to about ``budget_s`` seconds; return (samples/s, sample description)."""
+    import numpy as np
+
+    from dpt_b200.geometry import DetectorGeometry
+    from dpt_b200.plan import plan_rays
+    from oracle import oracle as O
+
+    panel = geometry.views[view]
+    rows, cols = panel.shape
+    pose = np.asarray((1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0, 0, 0, 0))
+
+    def block(first: int, count: int):
+        origin = tuple(panel.origin_mm[k] + first * panel.spacing_mm[1] * panel.v[k] for k in range(3))
+        sub = DetectorGeometry(panel.source_mm, origin, panel.u, panel.v, panel.spacing_mm, (count, cols))
+        plan = plan_rays(grid, sub)
+        lower, upper, _ = O.counts(plan, pose, samples=samples, threads=threads)
+        realised = int((upper > lower).sum()) * samples
+        seed = np.linspace(0.1, 1.0, plan.rays, dtype=np.float32)
+        start = time.perf_counter()
+        O.forward(plan, values, pose, samples=samples, threads=threads)
+        O.vjp(plan, values, pose, seed, samples=samples, flags=O.VJP_VOLUME | O.VJP_POSE12, threads=threads)
+        return realised, time.perf_counter() - start
+
+    centre = rows // 2
+    probe_rows = max(1, min(rows, 4))
+    realised, seconds = block(centre - probe_rows // 2, probe_rows)
+    rate = realised / max(seconds, 1e-9)
+    per_row = max(realised / probe_rows, 1.0)
+    want = int(max(1, min(rows, budget_s * rate / per_row)))
+    first = max(0, centre - want // 2)
+    realised, seconds = block(first, want)
+    sample = (f"view {view} of {len(geometry.views)}, detector rows {first}-{first + want - 1} of {rows} "
+              f"({want * cols} rays, {realised} realised ray-samples), forward + joint volume/pose VJP")
+    return realised / seconds, sample, seconds
+
+
+def run_gpu(args) -> None:
+    import numpy as np
+    import torch
+
+    rank, world, local = rank_info()
+    device = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=device)
+
+    from dpt_b200.torch import Projector
+    from dpt_b200.torch import _projection_ops as ops
+
+    grid, geometry, values, truth = build_workload(args, device)
+    dtype = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float16": torch.float16}[args.storage]
+    storage_bytes = 4 if args.storage == "float32" else 2
+    projector = Projector(grid=grid, geometry=geometry, precision="fp32", samples_per_ray=args.samples)
+    field = torch.tensor(values, device=device).to(dtype).contiguous()
+    views = len(geometry.views)
+    with torch.no_grad():
+        target = projector(field, truth)
+        noise = torch.Generator(device=device).manual_seed(args.seed + 2)
+        target += 0.01 * torch.randn(target.shape, generator=noise, device=device)
+    tangent = torch.zeros((views, 6), dtype=torch.float64, device=device)
+
+    def step(f, t, xi):
+        f = f.detach().requires_grad_(True)
+        xi = xi.detach().requires_grad_(True)
+        image = projector(f, xi)
+        residual = image - t
+        loss = 0.5 * (residual.double() * residual.double()).sum()
+        grad_field, grad_pose = torch.autograd.grad(loss, (f, xi))
+        if dist is not None:
+            dist.all_reduce(grad_field)
+        return loss.detach(), image.detach(), grad_field, grad_pose
+
+    # realised ray-samples of one step (identity tangent: the poses of the timed steps)
+    step(field, target, tangent)
+    ws = ops.workspace(field, projector.configuration, True, True)
+    identity = torch.tensor((1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0, 0, 0, 0), dtype=torch.float64,
+                            device=device).expand(views, 12).contiguous()
+    lower, upper, _ = ws.counts(identity)
+    nonempty = (upper > lower).reshape(views, -1).sum(dim=1).cpu().numpy().astype(np.int64)
+    realised_per_view = nonempty * args.samples
+    realised = int(realised_per_view.sum())
+    nominal = views * args.detector * args.detector * args.samples
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    for _ in range(args.warmup):
+        step(field, target, tangent)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    ws.launch_log = []
+    launches_before = ws.launches
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    stream = torch.cuda.current_stream()
+    spans = []
+    for _ in range(args.steps):
+        flush.zero_()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        step(field, target, tangent)
+        end.record(stream)
+        spans.append((start, end))
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    step_ms = sum(s.elapsed_time(e) for s, e in spans) / args.steps
+    gpu_launches = (ws.launches - launches_before)
+    log, ws.launch_log = ws.launch_log, None
+
+    # ---- per-kernel times (events around each C-ABI launch, on the launching stream)
+    per_kernel: dict[str, list[float]] = {}
+    per_kernel_samples: dict[str, list[int]] = {}
+    for name, first, count, start, end in log:
+        per_kernel.setdefault(name, []).append(start.elapsed_time(end))
+        per_kernel_samples.setdefault(name, []).append(int(realised_per_view[first:first + count].sum()))
+    totals = {name: sum(times) for name, times in per_kernel.items()}
+    dominant = max((k for k in totals if algorithmic_bytes(k, storage_bytes)), key=lambda k: totals[k])
+    peak, peak_kind = measured_peak()
+    launches = len(per_kernel[dominant])
+    mean_ms = totals[dominant] / launches
+    bytes_per_launch = algorithmic_bytes(dominant, storage_bytes) * sum(per_kernel_samples[dominant]) / launches
+    achieved = bytes_per_launch / (mean_ms * 1e-3) / 1e9
+    traffic_record = profile_traffic()
+    traffic = None
+    if traffic_record and traffic_record.get("kernel") == dominant:
+        traffic = traffic_record["dram_bytes_per_realised_sample"] * sum(per_kernel_samples[dominant]) / launches
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dominant,
+                "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
+                "kernel_ms": {k: round(v / args.steps, 3) for k, v in sorted(totals.items())}}
+
+    # ---- end to end through the public API with host buffers
+    host_field = field.cpu().pin_memory()
+    host_target = target.cpu().pin_memory()
+    host_tangent = tangent.cpu().pin_memory()
+    out_image = torch.empty(target.shape, dtype=target.dtype).pin_memory()
+    out_grad = torch.empty(field.shape, dtype=field.dtype).pin_memory()
+    out_pose = torch.empty(tangent.shape, dtype=torch.float64).pin_memory()
+    out_loss = torch.empty((), dtype=torch.float64).pin_memory()
+    h2d = host_field.numel() * host_field.element_size() + host_target.numel() * 4 + host_tangent.numel() * 8
+    d2h = out_image.numel() * 4 + out_grad.numel() * out_grad.element_size() + out_pose.numel() * 8 + 8
+
+    def e2e_step():
+        f = host_field.to(device, non_blocking=True)
+        t = host_target.to(device, non_blocking=True)
+        xi = host_tangent.to(device, non_blocking=True)
+        loss, image, gf, gp = step(f, t, xi)
+        out_loss.copy_(loss, non_blocking=True)
+        out_image.copy_(image, non_blocking=True)
+        out_grad.copy_(gf, non_blocking=True)
+        out_pose.copy_(gp, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e2e_spans = []
+    for _ in range(args.steps):
+        flush.zero_()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        e2e_step()
+        end.record(stream)
+        e2e_spans.append((start, end))
+    torch.cuda.synchronize()
+    e2e_ms = sum(s.elapsed_time(e) for s, e in e2e_spans) / args.steps
+
+    # max over ranks
+    if dist is not None:
+        timing = torch.tensor([step_ms, e2e_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(timing, op=dist.ReduceOp.MAX)
+        step_ms, e2e_ms = timing.tolist()
+        total = torch.tensor([realised], dtype=torch.float64, device=device)
+        dist.all_reduce(total)
+        realised_all = int(total.item())
+    else:
+        realised_all = realised
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, sample, seconds = oracle_sample_rate(grid, geometry, values, args.samples, 15.0, threads)
+        cpu_baseline = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                        "sample": sample + f"; {seconds:.1f} s on {threads} threads (C oracle -O3 -fopenmp)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": realised_all / (step_ms * 1e-3),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": step_ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if args.storage == "float32" else f"f32 ({args.storage} storage)",
+            "data": "synthetic (seeded chest-like HU phantom, 60 keV water model; no scanned volume)",
+            "config": {"workload": WORKLOAD if (args.size, args.views, args.detector, args.samples) == (256, 360, 512, 1024)
+                       else f"{args.size}^3, {args.views} views, {args.detector}^2, S={args.samples}",
+                       "grid": [args.size] * 3, "views_per_gpu": len(geometry.views),
+                       "detector": [args.detector, args.detector], "samples_per_ray": args.samples,
+                       "storage": args.storage, "precision": "fp32",
+                       "realised_ray_samples_per_step": realised_all,
+                       "nominal_ray_samples_per_step": nominal * world,
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"views sharded over {world} GPU(s), NCCL all-reduce of the volume gradient"
+                       if world > 1 else "1 GPU"},
+            "e2e": {"value": realised_all / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "gpu_launches": gpu_launches,
+            "roofline": roofline,
+            "cpu_baseline": cpu_baseline,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args) -> None:
+    """CPU restatement of the reference projector, timed on this host's cores."""
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    import torch
+
+    grid, geometry, values, _ = build_workload(args, torch.device("cpu"))
+    threads = os.cpu_count() or 1
+    budget = max(2.0, min(15.0, 150.0 / max(1, args.steps + args.warmup)))
+    for k in range(args.warmup):
+        oracle_sample_rate(grid, geometry, values, args.samples, budget, threads, view=k % len(geometry.views))
+    rates, seconds, sample = [], 0.0, ""
+    for k in range(args.steps):
+        rate, sample, took = oracle_sample_rate(grid, geometry, values, args.samples, budget, threads,
+                                                view=(37 * k) % len(geometry.views))
+        rates.append(rate)
+        seconds += took
+    value = statistics.fmean(rates)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * seconds / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
+        "data": "synthetic (seeded chest-like HU phantom, 60 keV water model; no scanned volume)",
+        "config": {"workload": WORKLOAD, "grid": [args.size] * 3, "views": args.views,
+                   "detector": [args.detector, args.detector], "samples_per_ray": args.samples,
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "per step: " + sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,437 @@
+// common.cuh - device arithmetic shared by the projector kernels.
+//
+// Floating-point contract: this code is compiled with -fmad=false.  Every fused
+// multiply-add is an explicit fma()/fmaf(); every other operation is one IEEE
+// rounding.  Where the reference projector (hcltech-robotics/dpt) writes
+// a*b + c*d this code computes fma(c, d, a*b); a + b*c is fma(b, c, a).  With
+// that contract the FP32 forward reproduces the reference sample sequence of
+// python/dpt/kernels/projection_fp32.py exactly, and the FP64 forward that of
+// python/dpt/kernels/projection.py.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+#include "../../include/dpt_b200.h"
+
+namespace dpt {
+
+constexpr int kBlock = 256;      // threads per block of the ray kernels
+constexpr int kTileCols = 16;    // detector columns per block tile
+constexpr int kTileRows = 16;    // detector rows per block tile
+
+struct Grid {
+    int nx, ny, nz;
+    double m[9];   // object_to_grid, row-major
+    double g0[3];  // grid origin (object mm)
+};
+
+// Kernel arguments passed by value (fits the 4 KB parameter space).
+struct RayArgs {
+    Grid grid;
+    int views;           // views in this launch
+    int view_begin;      // first absolute view of this launch
+    int rows, cols;      // rays per view = rows*cols
+    int samples;
+    int ray_kind;
+    int tiles_x;         // column tiles per view (panels)
+    int tiles_per_view;  // blocks per view
+    const double* poses;       // absolute view indexing
+    const double* view_table;  // absolute view indexing
+    const double* ray_sources;
+    const double* ray_endpoints;
+    int32_t* status;           // absolute view indexing
+};
+
+// ---------------------------------------------------------------- helpers
+
+__device__ __forceinline__ bool finite3(double a, double b, double c)
+{
+    return isfinite(a) && isfinite(b) && isfinite(c);
+}
+__device__ __forceinline__ bool finite3f(float a, float b, float c)
+{
+    return isfinite(a) && isfinite(b) && isfinite(c);
+}
+
+// r = A v, A row-major: fma(a2, v2, fma(a1, v1, a0*v0)).
+__device__ __forceinline__ void matvec(const double* a, const double* v, double* r)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        r[i] = fma(a[3 * i + 2], v[2], fma(a[3 * i + 1], v[1], a[3 * i] * v[0]));
+}
+
+// r = A^T v.
+__device__ __forceinline__ void matvec_t(const double* a, const double* v, double* r)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        r[i] = fma(a[6 + i], v[2], fma(a[3 + i], v[1], a[i] * v[0]));
+}
+
+// Ray index inside its view -> (pixel) for the tiled panel mapping, or the bundle index.
+// Returns false for padding threads.
+__device__ __forceinline__ bool ray_of_thread(const RayArgs& a, int tile, int* pixel)
+{
+    const int t = threadIdx.x;
+    if (a.ray_kind == DPT_RAYS_BUNDLE) {
+        const int index = tile * kBlock + t;
+        *pixel = index;
+        return index < a.rows * a.cols;
+    }
+    // 16x16 block tile; each warp covers 8 columns x 4 rows.
+    const int warp = t >> 5, lane = t & 31;
+    const int tile_row = tile / a.tiles_x, tile_col = tile - tile_row * a.tiles_x;
+    const int col = tile_col * kTileCols + (warp & 1) * 8 + (lane & 7);
+    const int row = tile_row * kTileRows + (warp >> 1) * 4 + (lane >> 3);
+    *pixel = row * a.cols + col;
+    return row < a.rows && col < a.cols;
+}
+
+// Source and endpoint (world mm) of ray `pixel` of absolute view `view`.
+__device__ __forceinline__ void ray_endpoints(const RayArgs& a, const double* w, int view, int pixel,
+                                              double* source, double* end)
+{
+    if (a.ray_kind == DPT_RAYS_BUNDLE) {
+        const int64_t ray = (int64_t)view * a.rows * a.cols + pixel;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            source[k] = __ldg(a.ray_sources + 3 * ray + k);
+            end[k] = __ldg(a.ray_endpoints + 3 * ray + k);
+        }
+        return;
+    }
+    const int r = pixel / a.cols;
+    const double row = (double)r, column = (double)(pixel - r * a.cols);
+    const int mode = (int)w[DPT_VIEW_MODE_WORD];
+    if (mode == DPT_PANEL_CONE) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            source[k] = w[k];
+            end[k] = fma(row, w[9 + k], fma(column, w[6 + k], w[3 + k]));
+        }
+    } else if (mode == DPT_PANEL_PARALLEL) {
+        const double cu = column * w[12], rv = row * w[13], length = w[14];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            end[k] = fma(rv, w[9 + k], fma(cu, w[6 + k], w[3 + k]));
+            source[k] = end[k] - length * w[k];
+        }
+    } else {
+        const double radius = w[14];
+        const double angle = column * w[12] / radius;
+        double s, c;
+        sincos(angle, &s, &c);
+        const double c1 = c - 1.0, sr = s * radius, rv = row * w[13];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            source[k] = w[k];
+            end[k] = fma(rv, w[9 + k], fma(sr, w[6 + k], fma(c1, w[15 + k], w[3 + k])));
+        }
+    }
+}
+
+// FP64 ray in grid-index coordinates (reference kernels/projection.py:79-102).
+struct Ray64 {
+    double origin[3], direction[3];
+    double os[3], od[3];    // object-frame source and direction
+    double wsr[3], wd[3];   // world source minus translation, world direction
+    double length;
+};
+
+__device__ __forceinline__ void ray_setup(const Grid& g, const double* pose, const double* source,
+                                          const double* end, Ray64& r)
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r.wsr[k] = source[k] - pose[9 + k];
+        r.wd[k] = end[k] - source[k];
+    }
+    matvec_t(pose, r.wsr, r.os);
+    matvec_t(pose, r.wd, r.od);
+    double rel[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) rel[k] = r.os[k] - g.g0[k];
+    matvec(g.m, rel, r.origin);
+    matvec(g.m, r.od, r.direction);
+    r.length = sqrt(fma(r.wd[2], r.wd[2], fma(r.wd[1], r.wd[1], r.wd[0] * r.wd[0])));
+}
+
+__device__ __forceinline__ bool valid_ray(const Ray64& r)
+{
+    return finite3(r.origin[0], r.origin[1], r.origin[2]) &&
+           finite3(r.direction[0], r.direction[1], r.direction[2]) &&
+           finite3(r.os[0], r.os[1], r.os[2]) && finite3(r.od[0], r.od[1], r.od[2]) &&
+           finite3(r.wsr[0], r.wsr[1], r.wsr[2]) && finite3(r.wd[0], r.wd[1], r.wd[2]) &&
+           isfinite(r.length) && r.length > 0.0;
+}
+
+// Slab clip of t in [0,1] against [-0.5, n-0.5] per axis with the active-face derivatives
+// (reference kernels/projection_fp32.py:78-109 and kernels/projection.py:147-184).
+template <typename T>
+struct Interval {
+    T lower, upper;
+    int lower_axis, upper_axis;  // -1: the segment end itself (no face derivative)
+    T lower_velocity, upper_velocity;
+
+    __device__ __forceinline__ void clip(const T* origin, const T* direction, int nx, int ny, int nz)
+    {
+        lower = T(0);
+        upper = T(1);
+        lower_axis = upper_axis = -1;
+        lower_velocity = upper_velocity = T(1);
+        const int shape[3] = {nx, ny, nz};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const T low = T(-0.5), high = T(shape[a]) - T(0.5), velocity = direction[a];
+            if (velocity == T(0)) {
+                if (origin[a] < low || origin[a] > high) upper = T(-1);
+            } else {
+                T first = (low - origin[a]) / velocity;
+                T last = (high - origin[a]) / velocity;
+                if (first > last) {
+                    const T t = first;
+                    first = last;
+                    last = t;
+                }
+                if (first > lower) {
+                    lower = first;
+                    lower_axis = a;
+                    lower_velocity = velocity;
+                }
+                if (last < upper) {
+                    upper = last;
+                    upper_axis = a;
+                    upper_velocity = velocity;
+                }
+            }
+        }
+    }
+
+    // d lower / d origin[a] = -1/v, d lower / d direction[a] = -lower/v on the active axis.
+    __device__ __forceinline__ void lower_gradients(T* og, T* dg) const
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) og[a] = dg[a] = T(0);
+        if (lower_axis >= 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                if (a == lower_axis) {
+                    og[a] = -T(1) / lower_velocity;
+                    dg[a] = -lower / lower_velocity;
+                }
+        }
+    }
+    __device__ __forceinline__ void upper_gradients(T* og, T* dg) const
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) og[a] = dg[a] = T(0);
+        if (upper_axis >= 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                if (a == upper_axis) {
+                    og[a] = -T(1) / upper_velocity;
+                    dg[a] = -upper / upper_velocity;
+                }
+        }
+    }
+};
+
+// Half-cell support test.
+__device__ __forceinline__ bool inside(float x, float y, float z, float hx, float hy, float hz)
+{
+    return x >= -0.5f && y >= -0.5f && z >= -0.5f && x <= hx && y <= hy && z <= hz;
+}
+__device__ __forceinline__ bool inside(double x, double y, double z, int nx, int ny, int nz)
+{
+    return x >= -0.5 && y >= -0.5 && z >= -0.5 && x <= (double)nx - 0.5 &&
+           y <= (double)ny - 0.5 && z <= (double)nz - 0.5;
+}
+
+// One axis of the clamped cell coordinate: lower = min(floor(clamp(p,0,n-1)), max(n-2,0)).
+struct Axis32 {
+    int lower;
+    float fraction;
+};
+__device__ __forceinline__ Axis32 axis32(float p, float high, int cap)
+{
+    const float value = fminf(fmaxf(p, 0.0f), high);
+    Axis32 r;
+    r.lower = min((int)floorf(value), cap);
+    r.fraction = value - (float)r.lower;
+    return r;
+}
+
+struct Axis64 {
+    int lower;
+    double fraction;
+};
+__device__ __forceinline__ Axis64 axis64(double p, double high, int cap)
+{
+    const double value = fmin(fmax(p, 0.0), high);
+    Axis64 r;
+    r.lower = min((int)floor(value), cap);
+    r.fraction = value - (double)r.lower;
+    return r;
+}
+
+// FP32 scatter increment: one rounded product, then |x| < 2^-126 flushed to signed zero
+// (reference kernels/projection_fp32.py:240-258; CUDA FP32 global atomics flush the same).
+__device__ __forceinline__ float scatter_increment(float factor, float weight)
+{
+    const float increment = factor * weight;
+    return fabsf(increment) < 0x1p-126f ? copysignf(0.0f, increment) : increment;
+}
+
+// Vector reduction of four FP32 values into 16-byte aligned global memory.
+__device__ __forceinline__ void red_add_v4(float* address, float a, float b, float c, float d)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(address), "f"(a), "f"(b),
+                 "f"(c), "f"(d)
+                 : "memory");
+}
+
+// ------------------------------------------------------------ field access
+
+// Corner-replicated copies of the field, written by the pack kernel.
+//  Quad (FP32): quad[(z*ny+y)*nx+x] = (v(x,y,z), v(x+1,y,z), v(x,y+1,z), v(x+1,y+1,z)),
+//               indices clamped to n-1 like corner_index.  A cell reads quad at z and at
+//               min(z+1, nz-1): corners 0-3 and 4-7.
+//  Octet (FP16/BF16): all eight corners of the cell at (x,y,z) in one 16-byte record.
+struct QuadF32 {
+    const float4* quad;
+    int nx, ny, nz;
+    __device__ __forceinline__ void load(int lx, int ly, int lz, float* v) const
+    {
+        const int64_t plane = (int64_t)nx * ny;
+        const int64_t base = (int64_t)ly * nx + lx;
+        const int64_t z1 = lz + 1 < nz ? lz + 1 : nz - 1;
+        const float4 a = __ldg(quad + (int64_t)lz * plane + base);
+        const float4 b = __ldg(quad + z1 * plane + base);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    }
+};
+
+struct PlainF32 {
+    const float* field;
+    int nx, ny, nz;
+    __device__ __forceinline__ void load(int lx, int ly, int lz, float* v) const
+    {
+        const int x1 = min(lx + 1, nx - 1), y1 = min(ly + 1, ny - 1), z1 = min(lz + 1, nz - 1);
+        const int64_t r00 = ((int64_t)lz * ny + ly) * nx, r10 = ((int64_t)lz * ny + y1) * nx;
+        const int64_t r01 = ((int64_t)z1 * ny + ly) * nx, r11 = ((int64_t)z1 * ny + y1) * nx;
+        v[0] = __ldg(field + r00 + lx); v[1] = __ldg(field + r00 + x1);
+        v[2] = __ldg(field + r10 + lx); v[3] = __ldg(field + r10 + x1);
+        v[4] = __ldg(field + r01 + lx); v[5] = __ldg(field + r01 + x1);
+        v[6] = __ldg(field + r11 + lx); v[7] = __ldg(field + r11 + x1);
+    }
+};
+
+template <bool kBF16>
+struct OctetHalf {
+    const uint4* octet;
+    int nx, ny, nz;
+    __device__ __forceinline__ void load(int lx, int ly, int lz, float* v) const
+    {
+        const uint4 r = __ldg(octet + ((int64_t)lz * ny + ly) * nx + lx);
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (kBF16) {
+                v[2 * k] = __uint_as_float(w[k] << 16);
+                v[2 * k + 1] = __uint_as_float(w[k] & 0xffff0000u);
+            } else {
+                const __half2 h = *reinterpret_cast<const __half2*>(&w[k]);
+                const float2 f = __half22float2(h);
+                v[2 * k] = f.x;
+                v[2 * k + 1] = f.y;
+            }
+        }
+    }
+};
+
+// Trilinear weight of corner c: (f0 f1) f2 with f = 1 - fraction for a 0 bit.
+__device__ __forceinline__ void corner_weights(float fx, float fy, float fz, float* w)
+{
+    const float ax = 1.0f - fx, ay = 1.0f - fy, az = 1.0f - fz;
+    w[0] = (ax * ay) * az;
+    w[1] = (fx * ay) * az;
+    w[2] = (ax * fy) * az;
+    w[3] = (fx * fy) * az;
+    w[4] = (ax * ay) * fz;
+    w[5] = (fx * ay) * fz;
+    w[6] = (ax * fy) * fz;
+    w[7] = (fx * fy) * fz;
+}
+
+// value = fmaf(w_c, v_c, value) over corners 0..7 from zero.
+__device__ __forceinline__ float interpolate(const float* w, const float* v)
+{
+    float value = fmaf(w[0], v[0], 0.0f);
+#pragma unroll
+    for (int c = 1; c < 8; ++c) value = fmaf(w[c], v[c], value);
+    return value;
+}
+
+// Grid-space slope of the FP32 pose path (reference kernels/projection_fp32.py:196-208).
+__device__ __forceinline__ void slope32(float fx, float fy, float fz, const float* v, float sx,
+                                        float sy, float sz, float* g)
+{
+    const float ax = 1.0f - fx, ay = 1.0f - fy, az = 1.0f - fz;
+    const float x0 = fmaf(fy, v[3] - v[2], ay * (v[1] - v[0]));
+    const float x1 = fmaf(fy, v[7] - v[6], ay * (v[5] - v[4]));
+    g[0] = sx * fmaf(fz, x1, az * x0);
+    const float y0 = fmaf(fx, v[3] - v[1], ax * (v[2] - v[0]));
+    const float y1 = fmaf(fx, v[7] - v[5], ax * (v[6] - v[4]));
+    g[1] = sy * fmaf(fz, y1, az * y0);
+    const float z0 = fmaf(fx, v[5] - v[1], ax * (v[4] - v[0]));
+    const float z1 = fmaf(fx, v[7] - v[3], ax * (v[6] - v[2]));
+    g[2] = sz * fmaf(fy, z1, ay * z0);
+}
+
+// FP64 weighted-lerp value (reference kernels/projection.py:249-260).
+__device__ __forceinline__ double interpolate64(double fx, double fy, double fz, const double* v)
+{
+    const double ax = 1.0 - fx, ay = 1.0 - fy, az = 1.0 - fz;
+    const double x00 = fma(fx, v[1], ax * v[0]), x10 = fma(fx, v[3], ax * v[2]);
+    const double x01 = fma(fx, v[5], ax * v[4]), x11 = fma(fx, v[7], ax * v[6]);
+    const double xy0 = fma(fy, x10, ay * x00), xy1 = fma(fy, x11, ay * x01);
+    return fma(fz, xy1, az * xy0);
+}
+
+// FP64 slope (reference kernels/projection.py:261-273).
+__device__ __forceinline__ void slope64(double fx, double fy, double fz, const double* v, double sx,
+                                        double sy, double sz, double* g)
+{
+    const double ax = 1.0 - fx, ay = 1.0 - fy, az = 1.0 - fz;
+    const double dx0 = fma(fy, v[3] - v[2], ay * (v[1] - v[0]));
+    const double dx1 = fma(fy, v[7] - v[6], ay * (v[5] - v[4]));
+    const double dy0 = fma(fx, v[3] - v[1], ax * (v[2] - v[0]));
+    const double dy1 = fma(fx, v[7] - v[5], ax * (v[6] - v[4]));
+    const double dz0 = fma(fx, v[5] - v[1], ax * (v[4] - v[0]));
+    const double dz1 = fma(fx, v[7] - v[3], ax * (v[6] - v[2]));
+    g[0] = sx * fma(fz, dx1, az * dx0);
+    g[1] = sy * fma(fz, dy1, az * dy0);
+    g[2] = sz * fma(fy, dz1, ay * dz0);
+}
+
+// Per-block staging of the view's pose (12 doubles) and panel record.
+struct ViewShared {
+    double pose[12];
+    double table[DPT_VIEW_WORDS];
+};
+
+__device__ __forceinline__ void stage_view(const RayArgs& a, int view, ViewShared& s)
+{
+    const int t = threadIdx.x;
+    if (t < 12) s.pose[t] = a.poses[12 * (int64_t)view + t];
+    if (a.ray_kind == DPT_RAYS_PANELS && t >= 32 && t < 32 + DPT_VIEW_WORDS)
+        s.table[t - 32] = a.view_table[(int64_t)view * DPT_VIEW_WORDS + (t - 32)];
+    __syncthreads();
+}
+
+}  // namespace dpt

@@ -1,0 +1,309 @@
+// forward.cu - optical depth and per-ray clip counts.
+//
+// One thread marches one ray; a 256-thread block covers a 16x16 detector tile (each warp
+// an 8x4 sub-tile) so the 32 rays of a warp sample neighbouring voxels at every step and
+// their corner loads share L1 lines.  One launch covers every view of a call (blockIdx.y
+// is the view), where the reference launches once per view.
+//
+// Arithmetic per mode (reference hcltech-robotics/dpt):
+//   F32  - python/dpt/kernels/projection_fp32.py:334-374 (FP64 setup, FP32 clip, fmaf
+//          midpoints, fmaf corner sum, serial FP32 total, total *= length*step)
+//   F64  - python/dpt/kernels/projection.py:802-846 with the midpoint integrator 770-799
+//   F32C - FP64 setup and clip; FP32 marching p_i = entry + (i+0.5) step_vector (the mixed
+//          recurrence of python/dpt/kernels/projection.py:368-392), FP32 corner sum and a
+//          compensated FP32 ray sum scaled by length*step in FP64.
+#include "launch.h"
+
+namespace dpt {
+namespace {
+
+struct FieldDims {
+    int nx, ny, nz;
+    float hx, hy, hz;   // n - 0.5 (support upper bound)
+    float mx, my, mz;   // n - 1 (clamp bound)
+    int cx, cy, cz;     // max(n - 2, 0) (lower-cell cap)
+    __device__ __forceinline__ void init(const Grid& g)
+    {
+        nx = g.nx; ny = g.ny; nz = g.nz;
+        hx = (float)nx - 0.5f; hy = (float)ny - 0.5f; hz = (float)nz - 0.5f;
+        mx = (float)(nx - 1); my = (float)(ny - 1); mz = (float)(nz - 1);
+        cx = max(nx - 2, 0); cy = max(ny - 2, 0); cz = max(nz - 2, 0);
+    }
+};
+
+// FP32 sample of the field at grid point (x, y, z): zero outside the half-cell support.
+template <class Field>
+__device__ __forceinline__ float sample32(const Field& f, const FieldDims& d, float x, float y,
+                                          float z)
+{
+    if (!inside(x, y, z, d.hx, d.hy, d.hz)) return 0.0f;
+    const Axis32 X = axis32(x, d.mx, d.cx), Y = axis32(y, d.my, d.cy), Z = axis32(z, d.mz, d.cz);
+    float v[8], w[8];
+    f.load(X.lower, Y.lower, Z.lower, v);
+    corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+    return interpolate(w, v);
+}
+
+template <class Field>
+__device__ __forceinline__ double sample64(const Field& f, const Grid& g, const double* p)
+{
+    if (!inside(p[0], p[1], p[2], g.nx, g.ny, g.nz)) return 0.0;
+    const Axis64 X = axis64(p[0], (double)(g.nx - 1), max(g.nx - 2, 0));
+    const Axis64 Y = axis64(p[1], (double)(g.ny - 1), max(g.ny - 2, 0));
+    const Axis64 Z = axis64(p[2], (double)(g.nz - 1), max(g.nz - 2, 0));
+    float v32[8];
+    f.load(X.lower, Y.lower, Z.lower, v32);
+    double v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = (double)v32[c];
+    return interpolate64(X.fraction, Y.fraction, Z.fraction, v);
+}
+
+template <typename Out>
+__device__ __forceinline__ bool finite_out(double value)
+{
+    return isfinite((Out)value);
+}
+
+template <int kArith, class Field, typename Out>
+__global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __restrict__ image)
+{
+    __shared__ ViewShared vs;
+    const int view_local = blockIdx.y;
+    const int view = a.view_begin + view_local;
+    stage_view(a, view, vs);
+    int pixel;
+    if (!ray_of_thread(a, blockIdx.x, &pixel)) return;
+
+    double source[3], end[3];
+    ray_endpoints(a, vs.table, view, pixel, source, end);
+    Ray64 r;
+    ray_setup(a.grid, vs.pose, source, end, r);
+    const int S = a.samples;
+    int bits = 0;
+    double result = 0.0;
+
+    if (kArith == DPT_ARITH_F32) {
+        const float o[3] = {(float)r.origin[0], (float)r.origin[1], (float)r.origin[2]};
+        const float d[3] = {(float)r.direction[0], (float)r.direction[1], (float)r.direction[2]};
+        const float length = (float)r.length;
+        if (!valid_ray(r) || !finite3f(o[0], o[1], o[2]) || !finite3f(d[0], d[1], d[2]) ||
+            !isfinite(length) || length <= 0.0f) {
+            bits = 2;
+        } else {
+            Interval<float> iv;
+            iv.clip(o, d, a.grid.nx, a.grid.ny, a.grid.nz);
+            float total = 0.0f;
+            if (iv.upper > iv.lower) {
+                FieldDims dims;
+                dims.init(a.grid);
+                const float step = (iv.upper - iv.lower) / (float)S;
+                bool finite = true;
+#pragma unroll 4
+                for (int i = 0; i < S; ++i) {
+                    const float position = fmaf((float)i + 0.5f, step, iv.lower);
+                    const float x = fmaf(position, d[0], o[0]);
+                    const float y = fmaf(position, d[1], o[1]);
+                    const float z = fmaf(position, d[2], o[2]);
+                    finite = finite && finite3f(x, y, z);
+                    total = total + sample32(f, dims, x, y, z);
+                }
+                if (!finite) bits |= 2;
+                total = total * (length * step);
+            }
+            if (!isfinite(total)) bits |= 2;
+            result = total;
+        }
+    } else if (kArith == DPT_ARITH_F64) {
+        if (!valid_ray(r)) {
+            bits = 2;
+        } else {
+            Interval<double> iv;
+            iv.clip(r.origin, r.direction, a.grid.nx, a.grid.ny, a.grid.nz);
+            double integral = 0.0;
+            if (iv.upper > iv.lower) {
+                const double step = (iv.upper - iv.lower) / (double)S;
+                bool finite = true;
+#pragma unroll 2
+                for (int i = 0; i < S; ++i) {
+                    const double position = fma((double)i + 0.5, step, iv.lower);
+                    double p[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) p[k] = fma(position, r.direction[k], r.origin[k]);
+                    finite = finite && finite3(p[0], p[1], p[2]);
+                    integral = integral + sample64(f, a.grid, p);
+                }
+                if (!finite) bits |= 2;
+                integral = integral * (r.length * step);
+            }
+            result = integral;
+            if (!finite_out<Out>(result)) bits |= 2;
+        }
+    } else {
+        if (!valid_ray(r)) {
+            bits = 2;
+        } else {
+            Interval<double> iv;
+            iv.clip(r.origin, r.direction, a.grid.nx, a.grid.ny, a.grid.nz);
+            if (iv.upper > iv.lower) {
+                FieldDims dims;
+                dims.init(a.grid);
+                const double step = (iv.upper - iv.lower) / (double)S;
+                float entry[3], sv[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
+                    sv[k] = (float)(step * r.direction[k]);
+                }
+                float sum = 0.0f, carry = 0.0f;
+                bool finite = true;
+#pragma unroll 4
+                for (int i = 0; i < S; ++i) {
+                    const float offset = (float)i + 0.5f;
+                    const float x = fmaf(offset, sv[0], entry[0]);
+                    const float y = fmaf(offset, sv[1], entry[1]);
+                    const float z = fmaf(offset, sv[2], entry[2]);
+                    finite = finite && finite3f(x, y, z);
+                    const float value = sample32(f, dims, x, y, z);
+                    const float yk = value - carry;
+                    const float t = sum + yk;
+                    carry = (t - sum) - yk;
+                    sum = t;
+                }
+                if (!finite) bits |= 2;
+                result = ((double)sum - (double)carry) * (r.length * step);
+            }
+            if (!finite_out<Out>(result)) bits |= 2;
+        }
+    }
+    const int64_t rays_per_view = (int64_t)a.rows * a.cols;
+    image[view_local * rays_per_view + pixel] = (Out)result;
+    if (bits) atomicOr(a.status + view, bits);
+}
+
+// Per-ray interval and number of midpoints inside the support, in each mode's arithmetic.
+template <int kArith>
+__global__ void __launch_bounds__(kBlock) k_counts(RayArgs a, double* __restrict__ lower,
+                                                   double* __restrict__ upper,
+                                                   int32_t* __restrict__ realised)
+{
+    __shared__ ViewShared vs;
+    const int view_local = blockIdx.y;
+    const int view = a.view_begin + view_local;
+    stage_view(a, view, vs);
+    int pixel;
+    if (!ray_of_thread(a, blockIdx.x, &pixel)) return;
+    double source[3], end[3];
+    ray_endpoints(a, vs.table, view, pixel, source, end);
+    Ray64 r;
+    ray_setup(a.grid, vs.pose, source, end, r);
+    const int S = a.samples;
+    int count = 0;
+    double lo = 0.0, hi = -1.0;
+    FieldDims dims;
+    dims.init(a.grid);
+    if (kArith == DPT_ARITH_F32) {
+        const float o[3] = {(float)r.origin[0], (float)r.origin[1], (float)r.origin[2]};
+        const float d[3] = {(float)r.direction[0], (float)r.direction[1], (float)r.direction[2]};
+        const float length = (float)r.length;
+        if (valid_ray(r) && finite3f(o[0], o[1], o[2]) && finite3f(d[0], d[1], d[2]) &&
+            isfinite(length) && length > 0.0f) {
+            Interval<float> iv;
+            iv.clip(o, d, a.grid.nx, a.grid.ny, a.grid.nz);
+            lo = iv.lower;
+            hi = iv.upper;
+            if (iv.upper > iv.lower) {
+                const float step = (iv.upper - iv.lower) / (float)S;
+                for (int i = 0; i < S; ++i) {
+                    const float position = fmaf((float)i + 0.5f, step, iv.lower);
+                    count += inside(fmaf(position, d[0], o[0]), fmaf(position, d[1], o[1]),
+                                    fmaf(position, d[2], o[2]), dims.hx, dims.hy, dims.hz);
+                }
+            }
+        }
+    } else if (valid_ray(r)) {
+        Interval<double> iv;
+        iv.clip(r.origin, r.direction, a.grid.nx, a.grid.ny, a.grid.nz);
+        lo = iv.lower;
+        hi = iv.upper;
+        if (iv.upper > iv.lower) {
+            const double step = (iv.upper - iv.lower) / (double)S;
+            if (kArith == DPT_ARITH_F64) {
+                for (int i = 0; i < S; ++i) {
+                    const double position = fma((double)i + 0.5, step, iv.lower);
+                    count += inside(fma(position, r.direction[0], r.origin[0]),
+                                    fma(position, r.direction[1], r.origin[1]),
+                                    fma(position, r.direction[2], r.origin[2]), a.grid.nx,
+                                    a.grid.ny, a.grid.nz);
+                }
+            } else {
+                float entry[3], sv[3];
+                for (int k = 0; k < 3; ++k) {
+                    entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
+                    sv[k] = (float)(step * r.direction[k]);
+                }
+                for (int i = 0; i < S; ++i) {
+                    const float offset = (float)i + 0.5f;
+                    count += inside(fmaf(offset, sv[0], entry[0]), fmaf(offset, sv[1], entry[1]),
+                                    fmaf(offset, sv[2], entry[2]), dims.hx, dims.hy, dims.hz);
+                }
+            }
+        }
+    }
+    const int64_t index = view_local * (int64_t)a.rows * a.cols + pixel;
+    lower[index] = lo;
+    upper[index] = hi;
+    realised[index] = count;
+}
+
+template <int kArith, class Field>
+cudaError_t forward_with(const dpt_problem& p, const RayArgs& a, const Field& f, void* image,
+                         dim3 grid, cudaStream_t stream)
+{
+    if (p.image_dtype == DPT_F64)
+        k_forward<kArith, Field, double><<<grid, kBlock, 0, stream>>>(a, f, static_cast<double*>(image));
+    else
+        k_forward<kArith, Field, float><<<grid, kBlock, 0, stream>>>(a, f, static_cast<float*>(image));
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_forward(const dpt_problem& p, const RayArgs& a, const void* packed, void* image,
+                           cudaStream_t stream)
+{
+    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    if (p.field_dtype == DPT_F32) {
+        if (p.layout == DPT_LAYOUT_DIRECT) {
+            PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
+            if (p.arith == DPT_ARITH_F32) return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
+            if (p.arith == DPT_ARITH_F64) return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
+            return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
+        }
+        QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+        if (p.arith == DPT_ARITH_F32) return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
+        if (p.arith == DPT_ARITH_F64) return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
+        return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
+    }
+    if (p.field_dtype == DPT_BF16) {
+        OctetHalf<true> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
+        return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
+    }
+    OctetHalf<false> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
+    return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
+}
+
+cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower, double* upper,
+                          int32_t* realised, cudaStream_t stream)
+{
+    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    if (p.arith == DPT_ARITH_F32)
+        k_counts<DPT_ARITH_F32><<<grid, kBlock, 0, stream>>>(a, lower, upper, realised);
+    else if (p.arith == DPT_ARITH_F64)
+        k_counts<DPT_ARITH_F64><<<grid, kBlock, 0, stream>>>(a, lower, upper, realised);
+    else
+        k_counts<DPT_ARITH_F32C><<<grid, kBlock, 0, stream>>>(a, lower, upper, realised);
+    return cudaGetLastError();
+}
+
+}  // namespace dpt

@@ -1,0 +1,33 @@
+// launch.h - host launchers shared between the kernel translation units and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/dpt_b200.h"
+#include "common.cuh"
+
+namespace dpt {
+
+// Fill a RayArgs record for views [view_begin, view_begin + view_count).
+RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status);
+
+// Blocks per view for the ray kernels.
+int tiles_per_view(const dpt_problem& p, int* tiles_x);
+
+cudaError_t launch_prepare_field(const dpt_problem& p, const void* field, void* packed,
+                                 const double* poses, int32_t* status, cudaStream_t stream);
+cudaError_t launch_forward(const dpt_problem& p, const RayArgs& a, const void* packed, void* image,
+                           cudaStream_t stream);
+cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower, double* upper,
+                          int32_t* realised, cudaStream_t stream);
+cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packed,
+                       const void* cotangent, int flags, float* accumulator, double* partials,
+                       cudaStream_t stream);
+cudaError_t launch_finish_pose(int view_begin, int view_count, int tiles, int components,
+                               const double* partials, double* gradient, int accumulate,
+                               int32_t* status, cudaStream_t stream);
+cudaError_t launch_fold(const dpt_problem& p, float* accumulator, double* total,
+                        int accumulate_total, void* gradient, int gradient_dtype, int clear,
+                        int32_t* status, cudaStream_t stream);
+
+}  // namespace dpt

@@ -1,0 +1,586 @@
+// vjp.cu - discrete VJP of the projector: volume cotangent and rigid-pose cotangent.
+//
+// Samples are recomputed exactly as in the forward (no per-sample state is stored).
+//
+// Volume: while consecutive samples of a ray stay in one interpolation cell their eight
+// corner increments accumulate in registers (the cell-run aggregation of the reference,
+// python/dpt/kernels/projection_fp32.py:459-548); when the ray leaves the cell the eight
+// sums go to a per-cell accumulator record of 32 bytes with two 16-byte vector reductions
+// (red.global.add.v4.f32) instead of eight scalar atomics.  The fold kernel (reduce.cu)
+// later gathers each voxel's corner slots, so the accumulator needs no atomics on voxels
+// shared by neighbouring cells.
+//
+// Pose: per ray the moments of the reference (mean, sum grad, sum t grad, the two clip
+// shifts) are accumulated in the sample arithmetic, chained through the clip-face
+// derivatives and M^T in FP64 (python/dpt/kernels/projection_fp32.py:549-602,
+// python/dpt/kernels/projection.py:1140-1217), then reduced per block with a fixed
+// warp-shuffle tree into FP64 partials that finish_pose reduces per view.
+#include "launch.h"
+
+namespace dpt {
+namespace {
+
+struct Dims {
+    int nx, ny, nz;
+    float hx, hy, hz, mx, my, mz;
+    int cx, cy, cz;
+    __device__ __forceinline__ void init(const Grid& g)
+    {
+        nx = g.nx; ny = g.ny; nz = g.nz;
+        hx = (float)nx - 0.5f; hy = (float)ny - 0.5f; hz = (float)nz - 0.5f;
+        mx = (float)(nx - 1); my = (float)(ny - 1); mz = (float)(nz - 1);
+        cx = max(nx - 2, 0); cy = max(ny - 2, 0); cz = max(nz - 2, 0);
+    }
+};
+
+__device__ __forceinline__ void flush_cell(float* acc, int cell, const float* cs)
+{
+    float* slot = acc + 8 * (int64_t)cell;
+    red_add_v4(slot, cs[0], cs[1], cs[2], cs[3]);
+    red_add_v4(slot + 4, cs[4], cs[5], cs[6], cs[7]);
+}
+
+// Pose outputs from the source/direction adjoints (FP64).
+//   mode 12: packed rows d L / d R[row][col] = wsr[row] sa[col] + wd[row] da[col] and
+//            d L / d t = -(R sa)   (reference kernels/projection_fp32.py:584-593)
+//   mode 6 / -6: local-right tangent (-sa, sa x os + da x od)  (reference kernels/geometry.py:24-52)
+__device__ __forceinline__ void pose_rows(int mode, const Ray64& r, const double* pose,
+                                          const double* sa, const double* da, double* g)
+{
+    if (mode == 12) {
+#pragma unroll
+        for (int row = 0; row < 3; ++row)
+#pragma unroll
+            for (int col = 0; col < 3; ++col)
+                g[3 * row + col] = fma(r.wd[row], da[col], r.wsr[row] * sa[col]);
+        double t[3];
+        matvec(pose, sa, t);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) g[9 + k] = -t[k];
+    } else {
+        const double* os = r.os;
+        const double* od = r.od;
+        g[0] = -sa[0];
+        g[1] = -sa[1];
+        g[2] = -sa[2];
+        g[3] = fma(-da[2], od[1], da[1] * od[2]) + fma(-sa[2], os[1], sa[1] * os[2]);
+        g[4] = fma(-da[0], od[2], da[2] * od[0]) + fma(-sa[0], os[2], sa[2] * os[0]);
+        g[5] = fma(-da[1], od[0], da[0] * od[1]) + fma(-sa[1], os[0], sa[0] * os[1]);
+    }
+}
+
+template <int kArith, class Field, bool kVol, bool kPose, typename Seed>
+__global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
+                                                int mode, float* __restrict__ acc,
+                                                double* __restrict__ partials)
+{
+    __shared__ ViewShared vs;
+    __shared__ double warp_sums[kBlock / 32][12];
+    const int view_local = blockIdx.y;
+    const int view = a.view_begin + view_local;
+    stage_view(a, view, vs);
+    int pixel;
+    const bool active = ray_of_thread(a, blockIdx.x, &pixel);
+    const int64_t rays_per_view = (int64_t)a.rows * a.cols;
+    const int S = a.samples;
+    double g[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) g[k] = 0.0;
+    int bits = 0;
+
+    if (active) {
+        double source[3], end[3];
+        ray_endpoints(a, vs.table, view, pixel, source, end);
+        Ray64 r;
+        ray_setup(a.grid, vs.pose, source, end, r);
+        const double seed_in = (double)cot[view_local * rays_per_view + pixel];
+        Dims dims;
+        dims.init(a.grid);
+
+        if (kArith == DPT_ARITH_F32) {
+            const float o[3] = {(float)r.origin[0], (float)r.origin[1], (float)r.origin[2]};
+            const float d[3] = {(float)r.direction[0], (float)r.direction[1], (float)r.direction[2]};
+            const float length = (float)r.length;
+            if (!valid_ray(r) || !finite3f(o[0], o[1], o[2]) || !finite3f(d[0], d[1], d[2]) ||
+                !isfinite(length) || length <= 0.0f) {
+                bits = 2;
+            } else {
+                Interval<float> iv;
+                iv.clip(o, d, dims.nx, dims.ny, dims.nz);
+                const float span = iv.upper - iv.lower;
+                const float seed = (float)seed_in;
+                if (!isfinite(seed)) bits |= 2;
+                if (span > 0.0f && seed != 0.0f) {
+                    const float step = span / (float)S;
+                    const float physical_step = length * step;
+                    const float vf = seed * physical_step;
+                    const bool bounded = isfinite(vf) && fabsf(vf) <= 1.0f;
+                    float mean = 0.0f, dO[3] = {0.0f, 0.0f, 0.0f}, dD[3] = {0.0f, 0.0f, 0.0f};
+                    float sl = 0.0f, su = 0.0f;
+                    float cs[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                    int pending = -1;
+                    bool finite = true;
+#pragma unroll 2
+                    for (int i = 0; i < S; ++i) {
+                        const float position = fmaf((float)i + 0.5f, step, iv.lower);
+                        const float x = fmaf(position, d[0], o[0]);
+                        const float y = fmaf(position, d[1], o[1]);
+                        const float z = fmaf(position, d[2], o[2]);
+                        finite = finite && finite3f(x, y, z);
+                        const bool in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                        Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
+                        float w[8];
+                        if (in) {
+                            X = axis32(x, dims.mx, dims.cx);
+                            Y = axis32(y, dims.my, dims.cy);
+                            Z = axis32(z, dims.mz, dims.cz);
+                            corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+                        }
+                        if (kPose) {
+                            float value = 0.0f, gs[3] = {0.0f, 0.0f, 0.0f};
+                            if (in) {
+                                float v[8];
+                                f.load(X.lower, Y.lower, Z.lower, v);
+                                value = interpolate(w, v);
+                                const float sx = (x >= 0.0f && x < dims.mx) ? 1.0f : 0.0f;
+                                const float sy = (y >= 0.0f && y < dims.my) ? 1.0f : 0.0f;
+                                const float sz = (z >= 0.0f && z < dims.mz) ? 1.0f : 0.0f;
+                                slope32(X.fraction, Y.fraction, Z.fraction, v, sx, sy, sz, gs);
+                            }
+                            mean = mean + value;
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                dO[k] = dO[k] + gs[k];
+                                dD[k] = fmaf(position, gs[k], dD[k]);
+                            }
+                            const float alpha = ((float)i + 0.5f) / (float)S;
+                            const float along = fmaf(gs[2], d[2], fmaf(gs[1], d[1], gs[0] * d[0]));
+                            sl = fmaf(1.0f - alpha, along, sl);
+                            su = fmaf(alpha, along, su);
+                        }
+                        if (kVol) {
+                            if (in) {
+                                const int cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
+                                if (cell != pending) {
+                                    if (pending >= 0) flush_cell(acc, pending, cs);
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                                    pending = cell;
+                                }
+                                if (bounded) {
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c)
+                                        cs[c] = cs[c] + scatter_increment(vf, w[c]);
+                                } else {
+                                    float* slot = acc + 8 * (int64_t)cell;
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c) {
+                                        const float inc = scatter_increment(vf, w[c]);
+                                        if (!isfinite(inc)) {
+                                            bits |= 2;
+                                            atomicAdd(slot + c, inc);
+                                        } else {
+                                            const float partial = cs[c] + inc;
+                                            if (!isfinite(partial)) {
+                                                atomicAdd(slot + c, cs[c]);
+                                                cs[c] = inc;
+                                            } else {
+                                                cs[c] = partial;
+                                            }
+                                        }
+                                    }
+                                }
+                            } else if (pending >= 0) {
+                                flush_cell(acc, pending, cs);
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                                pending = -1;
+                            }
+                        }
+                    }
+                    if (kVol && pending >= 0) flush_cell(acc, pending, cs);
+                    if (!finite) bits |= 2;
+                    if (kPose) {
+                        float lo_o[3], lo_d[3], up_o[3], up_d[3];
+                        iv.lower_gradients(lo_o, lo_d);
+                        iv.upper_gradients(up_o, up_d);
+                        const float lower_seed = fmaf(span, sl, -mean);
+                        const float upper_seed = fmaf(span, su, mean);
+                        double og[3], dg[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            og[k] = (double)fmaf(upper_seed, up_o[k], fmaf(lower_seed, lo_o[k], span * dO[k]));
+                            dg[k] = (double)fmaf(upper_seed, up_d[k], fmaf(lower_seed, lo_d[k], span * dD[k]));
+                        }
+                        const double factor = (double)((seed * length) / (float)S);
+                        double sa[3], da[3];
+                        matvec_t(a.grid.m, og, sa);
+                        matvec_t(a.grid.m, dg, da);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            sa[k] = factor * sa[k];
+                            da[k] = factor * da[k];
+                        }
+                        pose_rows(mode, r, vs.pose, sa, da, g);
+                    }
+                }
+            }
+        } else if (kArith == DPT_ARITH_F64) {
+            if (!valid_ray(r)) {
+                bits = 2;
+            } else {
+                Interval<double> iv;
+                iv.clip(r.origin, r.direction, dims.nx, dims.ny, dims.nz);
+                double span = iv.upper - iv.lower;
+                const double seed = seed_in;
+                if (!isfinite(seed)) bits |= 2;
+                if (seed == 0.0) span = 0.0;
+                if (span > 0.0) {
+                    double factor = seed * r.length;
+                    const double step = span / (double)S;
+                    const double vf = factor * span / (double)S;
+                    const bool power_of_two = (S & (S - 1)) == 0;
+                    const double inverse_samples = power_of_two ? 1.0 / (double)S : 0.0;
+                    double mean = 0.0, dO[3] = {0.0, 0.0, 0.0}, dD[3] = {0.0, 0.0, 0.0};
+                    double sl = 0.0, su = 0.0;
+                    double cs[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) cs[c] = 0.0;
+                    int pending = -1;
+                    bool finite = true;
+                    for (int i = 0; i < S; ++i) {
+                        const double alpha = power_of_two ? ((double)i + 0.5) * inverse_samples
+                                                          : ((double)i + 0.5) / (double)S;
+                        const double position = fma((double)i + 0.5, step, iv.lower);
+                        double p[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) p[k] = fma(position, r.direction[k], r.origin[k]);
+                        finite = finite && finite3(p[0], p[1], p[2]);
+                        const bool in = inside(p[0], p[1], p[2], dims.nx, dims.ny, dims.nz);
+                        Axis64 X{0, 0.0}, Y{0, 0.0}, Z{0, 0.0};
+                        if (in) {
+                            X = axis64(p[0], (double)(dims.nx - 1), dims.cx);
+                            Y = axis64(p[1], (double)(dims.ny - 1), dims.cy);
+                            Z = axis64(p[2], (double)(dims.nz - 1), dims.cz);
+                        }
+                        if (kPose) {
+                            double value = 0.0, gs[3] = {0.0, 0.0, 0.0};
+                            if (in) {
+                                float v32[8];
+                                f.load(X.lower, Y.lower, Z.lower, v32);
+                                double v[8];
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) v[c] = (double)v32[c];
+                                value = interpolate64(X.fraction, Y.fraction, Z.fraction, v);
+                                const double sx = (p[0] >= 0.0 && p[0] < (double)(dims.nx - 1)) ? 1.0 : 0.0;
+                                const double sy = (p[1] >= 0.0 && p[1] < (double)(dims.ny - 1)) ? 1.0 : 0.0;
+                                const double sz = (p[2] >= 0.0 && p[2] < (double)(dims.nz - 1)) ? 1.0 : 0.0;
+                                slope64(X.fraction, Y.fraction, Z.fraction, v, sx, sy, sz, gs);
+                            }
+                            mean = mean + value;
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                dO[k] = dO[k] + gs[k];
+                                dD[k] = fma(position, gs[k], dD[k]);
+                            }
+                            const double along =
+                                fma(gs[2], r.direction[2], fma(gs[1], r.direction[1], gs[0] * r.direction[0]));
+                            sl = fma(1.0 - alpha, along, sl);
+                            su = fma(alpha, along, su);
+                        }
+                        if (kVol) {
+                            if (in) {
+                                const int cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
+                                if (cell != pending) {
+                                    if (pending >= 0) {
+                                        float c32[8];
+#pragma unroll
+                                        for (int c = 0; c < 8; ++c) c32[c] = (float)cs[c];
+                                        flush_cell(acc, pending, c32);
+                                    }
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c) cs[c] = 0.0;
+                                    pending = cell;
+                                }
+                                const double fx = X.fraction, fy = Y.fraction, fz = Z.fraction;
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) {
+                                    double contribution = vf * ((c & 1) ? fx : 1.0 - fx);
+                                    contribution = contribution * ((c & 2) ? fy : 1.0 - fy);
+                                    contribution = contribution * ((c & 4) ? fz : 1.0 - fz);
+                                    const float rounded = (float)contribution;
+                                    if (!isfinite(rounded)) bits |= 2;
+                                    cs[c] = cs[c] + (double)rounded;
+                                }
+                            } else if (pending >= 0) {
+                                float c32[8];
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) {
+                                    c32[c] = (float)cs[c];
+                                    cs[c] = 0.0;
+                                }
+                                flush_cell(acc, pending, c32);
+                                pending = -1;
+                            }
+                        }
+                    }
+                    if (kVol && pending >= 0) {
+                        float c32[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) c32[c] = (float)cs[c];
+                        flush_cell(acc, pending, c32);
+                    }
+                    if (!finite) bits |= 2;
+                    if (kPose) {
+                        double lo_o[3], lo_d[3], up_o[3], up_d[3];
+                        iv.lower_gradients(lo_o, lo_d);
+                        iv.upper_gradients(up_o, up_d);
+                        const double lower_seed = fma(span, sl, -mean);
+                        const double upper_seed = fma(span, su, mean);
+                        double og[3], dg[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            og[k] = fma(upper_seed, up_o[k], fma(lower_seed, lo_o[k], span * dO[k]));
+                            dg[k] = fma(upper_seed, up_d[k], fma(lower_seed, lo_d[k], span * dD[k]));
+                        }
+                        factor = factor / (double)S;
+                        double sa[3], da[3];
+                        matvec_t(a.grid.m, og, sa);
+                        matvec_t(a.grid.m, dg, da);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            sa[k] = factor * sa[k];
+                            da[k] = factor * da[k];
+                        }
+                        pose_rows(mode, r, vs.pose, sa, da, g);
+                    }
+                }
+            }
+        } else {
+            // F32C: FP64 clip, FP32 marching and sample arithmetic, pose moments
+            // G = sum grad and H = sum alpha grad with the integral, chained in FP64.
+            if (!valid_ray(r)) {
+                bits = 2;
+            } else {
+                Interval<double> iv;
+                iv.clip(r.origin, r.direction, dims.nx, dims.ny, dims.nz);
+                const double span = iv.upper - iv.lower;
+                const double seed = seed_in;
+                if (!isfinite(seed)) bits |= 2;
+                if (span > 0.0 && seed != 0.0) {
+                    const double step = span / (double)S;
+                    const float vf = (float)(seed * r.length * step);
+                    const bool bounded = isfinite(vf) && fabsf(vf) <= 1.0f;
+                    float entry[3], sv[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
+                        sv[k] = (float)(step * r.direction[k]);
+                    }
+                    const float inv_s = 1.0f / (float)S;
+                    float mean = 0.0f, carry = 0.0f, G[3] = {0.0f, 0.0f, 0.0f}, H[3] = {0.0f, 0.0f, 0.0f};
+                    float cs[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                    int pending = -1;
+                    bool finite = true;
+#pragma unroll 2
+                    for (int i = 0; i < S; ++i) {
+                        const float offset = (float)i + 0.5f;
+                        const float x = fmaf(offset, sv[0], entry[0]);
+                        const float y = fmaf(offset, sv[1], entry[1]);
+                        const float z = fmaf(offset, sv[2], entry[2]);
+                        finite = finite && finite3f(x, y, z);
+                        const bool in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                        Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
+                        float w[8];
+                        if (in) {
+                            X = axis32(x, dims.mx, dims.cx);
+                            Y = axis32(y, dims.my, dims.cy);
+                            Z = axis32(z, dims.mz, dims.cz);
+                            corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+                        }
+                        if (kPose) {
+                            float value = 0.0f, gs[3] = {0.0f, 0.0f, 0.0f};
+                            if (in) {
+                                float v[8];
+                                f.load(X.lower, Y.lower, Z.lower, v);
+                                value = interpolate(w, v);
+                                const float sx = (x >= 0.0f && x < dims.mx) ? 1.0f : 0.0f;
+                                const float sy = (y >= 0.0f && y < dims.my) ? 1.0f : 0.0f;
+                                const float sz = (z >= 0.0f && z < dims.mz) ? 1.0f : 0.0f;
+                                slope32(X.fraction, Y.fraction, Z.fraction, v, sx, sy, sz, gs);
+                            }
+                            const float yk = value - carry;
+                            const float t = mean + yk;
+                            carry = (t - mean) - yk;
+                            mean = t;
+                            const float alpha = offset * inv_s;
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                G[k] = G[k] + gs[k];
+                                H[k] = fmaf(alpha, gs[k], H[k]);
+                            }
+                        }
+                        if (kVol) {
+                            if (in) {
+                                const int cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
+                                if (cell != pending) {
+                                    if (pending >= 0) flush_cell(acc, pending, cs);
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                                    pending = cell;
+                                }
+                                if (bounded) {
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c)
+                                        cs[c] = cs[c] + scatter_increment(vf, w[c]);
+                                } else {
+                                    float* slot = acc + 8 * (int64_t)cell;
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c) {
+                                        const float inc = scatter_increment(vf, w[c]);
+                                        if (!isfinite(inc)) bits |= 2;
+                                        atomicAdd(slot + c, inc);
+                                    }
+                                }
+                            } else if (pending >= 0) {
+                                flush_cell(acc, pending, cs);
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                                pending = -1;
+                            }
+                        }
+                    }
+                    if (kVol && pending >= 0) flush_cell(acc, pending, cs);
+                    if (!finite) bits |= 2;
+                    if (kPose) {
+                        const double* dr = r.direction;
+                        const double Gd[3] = {G[0], G[1], G[2]}, Hd[3] = {H[0], H[1], H[2]};
+                        const double mean64 = (double)mean - (double)carry;
+                        const double g_along = fma(Gd[2], dr[2], fma(Gd[1], dr[1], Gd[0] * dr[0]));
+                        const double h_along = fma(Hd[2], dr[2], fma(Hd[1], dr[1], Hd[0] * dr[0]));
+                        const double su = h_along, sl = g_along - h_along;
+                        const double lower_seed = fma(span, sl, -mean64);
+                        const double upper_seed = fma(span, su, mean64);
+                        double lo_o[3], lo_d[3], up_o[3], up_d[3];
+                        iv.lower_gradients(lo_o, lo_d);
+                        iv.upper_gradients(up_o, up_d);
+                        double og[3], dg[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const double direct_direction = fma(span, Hd[k], iv.lower * Gd[k]);
+                            og[k] = fma(upper_seed, up_o[k], fma(lower_seed, lo_o[k], span * Gd[k]));
+                            dg[k] = fma(upper_seed, up_d[k], fma(lower_seed, lo_d[k], span * direct_direction));
+                        }
+                        const double factor = seed * r.length / (double)S;
+                        double sa[3], da[3];
+                        matvec_t(a.grid.m, og, sa);
+                        matvec_t(a.grid.m, dg, da);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            sa[k] = factor * sa[k];
+                            da[k] = factor * da[k];
+                        }
+                        pose_rows(mode, r, vs.pose, sa, da, g);
+                    }
+                }
+            }
+        }
+    }
+
+    if (kPose) {
+        if (mode < 0) {
+            if (active) {
+                double* out = partials + 6 * (view_local * rays_per_view + pixel);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    out[k] = g[k];
+                    if (!isfinite(g[k])) bits |= 2;
+                }
+            }
+        } else {
+            const int components = mode;
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                if (k < components) {
+                    double v = g[k];
+#pragma unroll
+                    for (int offset = 16; offset > 0; offset >>= 1)
+                        v += __shfl_down_sync(0xffffffffu, v, offset);
+                    if (lane == 0) warp_sums[warp][k] = v;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < components) {
+                double total = 0.0;
+#pragma unroll
+                for (int w = 0; w < kBlock / 32; ++w) total += warp_sums[w][threadIdx.x];
+                partials[((int64_t)view_local * a.tiles_per_view + blockIdx.x) * components +
+                         threadIdx.x] = total;
+            }
+        }
+    }
+    if (bits) atomicOr(a.status + view, bits);
+}
+
+template <int kArith, class Field, typename Seed>
+cudaError_t vjp_with(const RayArgs& a, const Field& f, const Seed* cot, int flags, float* acc,
+                     double* partials, cudaStream_t stream)
+{
+    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const bool volume = (flags & DPT_VJP_VOLUME) != 0;
+    const bool pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
+    const int mode = (flags & DPT_VJP_POSE12) ? 12 : ((flags & DPT_VJP_PER_RAY6) ? -6 : 6);
+    if (volume && pose)
+        k_vjp<kArith, Field, true, true, Seed><<<grid, kBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+    else if (volume)
+        k_vjp<kArith, Field, true, false, Seed><<<grid, kBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+    else
+        k_vjp<kArith, Field, false, true, Seed><<<grid, kBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+    return cudaGetLastError();
+}
+
+template <int kArith, class Field>
+cudaError_t vjp_seed(const dpt_problem& p, const RayArgs& a, const Field& f, const void* cot,
+                     int flags, float* acc, double* partials, cudaStream_t stream)
+{
+    if (p.image_dtype == DPT_F64)
+        return vjp_with<kArith>(a, f, static_cast<const double*>(cot), flags, acc, partials, stream);
+    return vjp_with<kArith>(a, f, static_cast<const float*>(cot), flags, acc, partials, stream);
+}
+
+}  // namespace
+
+cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packed,
+                       const void* cotangent, int flags, float* accumulator, double* partials,
+                       cudaStream_t stream)
+{
+    if (p.field_dtype == DPT_F32) {
+        if (p.layout == DPT_LAYOUT_DIRECT) {
+            PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
+            if (p.arith == DPT_ARITH_F32)
+                return vjp_seed<DPT_ARITH_F32>(p, a, f, cotangent, flags, accumulator, partials, stream);
+            if (p.arith == DPT_ARITH_F64)
+                return vjp_seed<DPT_ARITH_F64>(p, a, f, cotangent, flags, accumulator, partials, stream);
+            return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        }
+        QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+        if (p.arith == DPT_ARITH_F32)
+            return vjp_seed<DPT_ARITH_F32>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        if (p.arith == DPT_ARITH_F64)
+            return vjp_seed<DPT_ARITH_F64>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
+    }
+    if (p.field_dtype == DPT_BF16) {
+        OctetHalf<true> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
+        return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
+    }
+    OctetHalf<false> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
+    return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
+}
+
+}  // namespace dpt

@@ -1,0 +1,450 @@
+"""Projection workspaces: device tables, scratch and checked calls over the C ABI.
+
+``ProjectionSpec`` and ``prepare_projection`` mirror the reference's lower-level
+operator layer (hcltech-robotics/dpt ``python/dpt/projection.py:67-140`` and
+``:526-622``); ``project_optical_depth``, ``projection_vjp`` and
+``projection_pose_sensitivities`` mirror ``:747-809``, ``:871-1018`` and
+``:1021-1084``.  Arrays are torch CUDA tensors and work is enqueued on the
+caller's current torch stream.
+
+A workspace owns, per device:
+
+* the panel table or ray bundle of its plan (uploaded once),
+* the corner-replicated copy of the last prepared field (reused while the same
+  tensor is passed again unchanged, tracked through torch's version counter),
+* the per-cell FP32 volume accumulator (kept zero between calls), an FP64 running
+  total for the widening of the volume gradient, FP64 pose partials,
+* one int32 status word per view and a pinned host copy for the checkpoint.
+
+Checked calls end with one status readback and a wait on the stream (the
+reference's ``StatusCheckpoint``, ``python/dpt/_runtime.py:318-446``); a nonzero
+word raises ``ContractError`` (bit 1), ``TrialDomainError`` (bit 8) or
+``NumericalError`` (bit 2), names the view and clears the words, so the next
+call starts clean.
+"""
+
+from __future__ import annotations
+
+import threading
+import weakref
+from dataclasses import dataclass
+from typing import Literal
+
+import torch
+
+from . import _native as N
+from .contracts import ContractError, NumericalError, integer, raise_device_status
+from .plan import RayPlan, plan_rays
+from .volumes import GridSpec
+
+SamplingPrecision = Literal["float32", "float64", "compensated"]
+StoragePrecision = Literal["float32", "float16", "bfloat16"]
+
+_STORAGE = {"float32": (N.F32, torch.float32), "float16": (N.F16, torch.float16),
+            "bfloat16": (N.BF16, torch.bfloat16)}
+_ARITH = {"float32": N.ARITH_F32, "float64": N.ARITH_F64, "compensated": N.ARITH_F32C}
+
+
+@dataclass(frozen=True, slots=True)
+class ProjectionSpec:
+    """Quadrature and arithmetic of one projector.
+
+    ``samples_per_ray`` midpoints per clipped ray.  ``sampling_precision``:
+    ``"float32"`` is the reference FP32 projector (FP64 ray setup, FP32 clip,
+    interpolation and serial ray sum), ``"float64"`` the reference strict FP64
+    projector, ``"compensated"`` FP64 setup and clip with FP32 marching,
+    interpolation and a compensated (Kahan) ray sum - the form used for FP16 and
+    BF16 storage.  ``precision`` is the image / cotangent dtype.
+    ``widen_views`` is how many views accumulate in FP32 before the volume
+    gradient is widened into its FP64 total (the reference uses 8 for FP32 and 2
+    for FP64 sampling).
+    """
+
+    samples_per_ray: int
+    active_pose: bool = True
+    active_volume: bool = False
+    precision: Literal["float32", "float64"] = "float32"
+    sampling_precision: SamplingPrecision = "float64"
+    storage_precision: StoragePrecision = "float32"
+    widen_views: int | None = None
+    layout: Literal["replicated", "direct"] = "replicated"
+
+    def __post_init__(self) -> None:
+        integer(self.samples_per_ray, "samples_per_ray", minimum=1)
+        if self.precision not in ("float32", "float64"):
+            raise ContractError("projection precision must be float32 or float64")
+        if self.sampling_precision not in _ARITH:
+            raise ContractError("sampling_precision must be float32, float64 or compensated")
+        if self.storage_precision not in _STORAGE:
+            raise ContractError("storage_precision must be float32, float16 or bfloat16")
+        if self.storage_precision != "float32" and self.sampling_precision != "compensated":
+            raise ContractError("FP16/BF16 storage requires compensated FP32 sampling")
+        if type(self.active_pose) is not bool or type(self.active_volume) is not bool:
+            raise ContractError("active input flags must be booleans")
+        if self.widen_views is not None:
+            integer(self.widen_views, "widen_views", minimum=1)
+        if self.layout not in ("replicated", "direct"):
+            raise ContractError("layout must be replicated or direct")
+        if self.layout == "direct" and self.storage_precision != "float32":
+            raise ContractError("the direct layout reads FP32 storage only")
+
+    @property
+    def arith(self) -> int:
+        return _ARITH[self.sampling_precision]
+
+    @property
+    def field_code(self) -> int:
+        return _STORAGE[self.storage_precision][0]
+
+    @property
+    def field_dtype(self) -> torch.dtype:
+        return _STORAGE[self.storage_precision][1]
+
+    @property
+    def image_code(self) -> int:
+        return N.F64 if self.precision == "float64" else N.F32
+
+    @property
+    def image_dtype(self) -> torch.dtype:
+        return torch.float64 if self.precision == "float64" else torch.float32
+
+    @property
+    def batch_views(self) -> int:
+        if self.widen_views is not None:
+            return self.widen_views
+        return 2 if self.sampling_precision == "float64" else 8
+
+
+def _ptr(tensor: torch.Tensor | None) -> int | None:
+    return None if tensor is None else tensor.data_ptr()
+
+
+def _stream(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class ProjectionWorkspace:
+    """Device state of one (grid, geometry, spec) on one CUDA device."""
+
+    def __init__(self, plan: RayPlan, spec: ProjectionSpec, device: torch.device | str) -> None:
+        device = torch.device(device)
+        if device.type != "cuda":
+            raise ContractError("the B200 projector runs on CUDA devices only")
+        if spec.sampling_precision != "float64" and max(plan.grid.shape) > 2**24:
+            raise ContractError("FP32 sampling requires grid axis counts at most 2**24")
+        N.library()
+        self.plan = plan
+        self.spec = spec
+        self.device = device
+        self.lock = threading.RLock()
+        self.problem = plan.problem(
+            spec.samples_per_ray,
+            spec.arith,
+            field_dtype=spec.field_code,
+            image_dtype=spec.image_code,
+            layout=N.LAYOUT_DIRECT if spec.layout == "direct" else N.LAYOUT_REPLICATED,
+        )
+        with torch.cuda.device(device):
+            self.view_table = (
+                torch.from_numpy(plan.view_table).to(device) if plan.view_table is not None else None
+            )
+            self.sources = torch.from_numpy(plan.sources).to(device) if plan.sources is not None else None
+            self.endpoints = (
+                torch.from_numpy(plan.endpoints).to(device) if plan.endpoints is not None else None
+            )
+            self.status = torch.zeros(plan.views, dtype=torch.int32, device=device)
+            self.status_host = torch.zeros(plan.views, dtype=torch.int32, pin_memory=True)
+        self._packed: torch.Tensor | None = None
+        self._packed_for: tuple | None = None
+        self._accumulator: torch.Tensor | None = None
+        self._total: torch.Tensor | None = None
+        self._partials: torch.Tensor | None = None
+        # Optional instrumentation: a list receiving (name, view_begin, view_count,
+        # start_event, end_event) per C-ABI call, and a count of C-ABI calls.
+        self.launch_log: list | None = None
+        self.launches = 0
+
+    # ------------------------------------------------------------ scratch
+    @property
+    def views(self) -> int:
+        return self.plan.views
+
+    def scratch_bytes(self) -> int:
+        total = 0
+        for tensor in (self._packed, self._accumulator, self._total, self._partials):
+            if tensor is not None:
+                total += tensor.numel() * tensor.element_size()
+        return total
+
+    def release_scratch(self) -> None:
+        """Drop the cached field copy and gradient scratch (allocated again on demand)."""
+        self._packed = self._packed_for = None
+        self._accumulator = self._total = self._partials = None
+
+    def _bytes(self, size: int) -> torch.Tensor:
+        # 256-byte aligned storage from the caching allocator
+        return torch.empty(max(size, 1), dtype=torch.uint8, device=self.device)
+
+    def accumulator(self) -> torch.Tensor:
+        if self._accumulator is None:
+            size = N.library().dpt_b200_accumulator_bytes(self.problem)
+            self._accumulator = torch.zeros(size // 4, dtype=torch.float32, device=self.device)
+        return self._accumulator
+
+    def total(self) -> torch.Tensor:
+        if self._total is None:
+            self._total = torch.empty(self.plan.grid.voxels, dtype=torch.float64, device=self.device)
+        return self._total
+
+    def partials(self) -> torch.Tensor:
+        size = N.library().dpt_b200_pose_partials_bytes(self.problem, self.views)
+        if self._partials is None or self._partials.numel() * 8 < size:
+            self._partials = torch.empty(max(size // 8, 1), dtype=torch.float64, device=self.device)
+        return self._partials
+
+    # ------------------------------------------------------------- inputs
+    def check_field(self, field: torch.Tensor) -> torch.Tensor:
+        if not isinstance(field, torch.Tensor):
+            raise ContractError("field must be a Torch tensor")
+        if field.device != self.device:
+            raise ContractError("field must be on the workspace device")
+        if field.dtype != self.spec.field_dtype:
+            raise ContractError(f"field must use {self.spec.storage_precision} storage")
+        if field.numel() != self.plan.grid.voxels or not field.is_contiguous():
+            raise ContractError("field must be contiguous with grid shape (nz,ny,nx)")
+        return field
+
+    def check_poses(self, poses: torch.Tensor) -> torch.Tensor:
+        if not isinstance(poses, torch.Tensor) or poses.dtype != torch.float64:
+            raise ContractError("poses must be a float64 Torch tensor")
+        if poses.device != self.device:
+            raise ContractError("poses must be on the workspace device")
+        if poses.numel() == 12 and self.views > 1:
+            poses = poses.reshape(1, 12).expand(self.views, 12)
+        if tuple(poses.shape) not in ((self.views, 12), (12,)) or poses.numel() != 12 * self.views:
+            raise ContractError(f"poses must have shape ({self.views}, 12)")
+        return poses.reshape(self.views, 12).contiguous()
+
+    def rays(self, poses: torch.Tensor, view_begin: int = 0, view_count: int | None = None) -> N.Rays:
+        r = N.Rays()
+        r.poses = poses.data_ptr()
+        r.view_table = _ptr(self.view_table)
+        r.ray_sources = _ptr(self.sources)
+        r.ray_endpoints = _ptr(self.endpoints)
+        r.view_begin = view_begin
+        r.view_count = self.views - view_begin if view_count is None else view_count
+        return r
+
+    def prepare_field(self, field: torch.Tensor, poses: torch.Tensor) -> torch.Tensor:
+        """Validate field and poses (status bits 8 and 1) and return the sampling layout."""
+        lib = N.library()
+        if self.spec.layout == "direct":
+            self._run("prepare_field", lambda: lib.dpt_b200_prepare_field(self.problem, field.data_ptr(), None, poses.data_ptr(),
+                                           self.status.data_ptr(), _stream(self.device)))
+            return field
+        if self._packed is not None and self._packed_for is not None:
+            ref, version, pointer = self._packed_for
+            if ref() is field and version == field._version and pointer == field.data_ptr():
+                # unchanged field: validate again (field and poses) without rewriting the copy
+                self._run("prepare_field", lambda: lib.dpt_b200_prepare_field(self.problem, field.data_ptr(), None,
+                                               poses.data_ptr(), self.status.data_ptr(),
+                                               _stream(self.device)))
+                return self._packed
+        size = lib.dpt_b200_packed_bytes(self.problem)
+        if self._packed is None or self._packed.numel() < size:
+            self._packed = self._bytes(size)
+        self._run("prepare_field", lambda: lib.dpt_b200_prepare_field(self.problem, field.data_ptr(), self._packed.data_ptr(),
+                                       poses.data_ptr(), self.status.data_ptr(), _stream(self.device)))
+        self._packed_for = (weakref.ref(field), field._version, field.data_ptr())
+        return self._packed
+
+    # ----------------------------------------------------------- launches
+    def _run(self, name: str, call, view_begin: int = 0, view_count: int | None = None) -> None:
+        """Make one C-ABI call; with ``launch_log`` set, bracket it with CUDA events."""
+        self.launches += 1
+        log = self.launch_log
+        if log is None:
+            N.check(call(), name)
+            return
+        stream = torch.cuda.current_stream(self.device)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        code = call()
+        end.record(stream)
+        N.check(code, name)
+        count = self.views - view_begin if view_count is None else view_count
+        log.append((name, view_begin, count, start, end))
+
+    # --------------------------------------------------------- checkpoint
+    def consume_status(self, operator: str = "projection") -> None:
+        """Read every status word once, raise the first typed error, clear the words."""
+        self.status_host.copy_(self.status, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        codes = self.status_host.tolist()
+        if any(codes):
+            self.status.zero_()
+            failures = []
+            for view, code in enumerate(codes):
+                if code:
+                    try:
+                        raise_device_status(code, operator)
+                    except (ContractError, NumericalError) as error:
+                        error.args = (f"{operator} view {view}: {error}", *error.args[1:])
+                        failures.append(error)
+            first = failures[0]
+            for view, code in enumerate(codes):
+                if code:
+                    first.add_note(f"view {view} status {code}")
+            raise first
+
+    # ------------------------------------------------------------ compute
+    def forward(self, field: torch.Tensor, poses: torch.Tensor, out: torch.Tensor | None = None,
+                *, checked: bool = True) -> torch.Tensor:
+        """Optical depth ``(views, rows, cols)`` (bundles: ``(rays,)``)."""
+        with self.lock, torch.cuda.device(self.device):
+            field = self.check_field(field)
+            poses = self.check_poses(poses)
+            if out is None:
+                out = torch.empty(self.plan.image_shape, dtype=self.spec.image_dtype, device=self.device)
+            elif (tuple(out.shape) != self.plan.image_shape or out.dtype != self.spec.image_dtype
+                  or out.device != self.device or not out.is_contiguous()):
+                raise ContractError("out must match the projector's shape, dtype and input device")
+            packed = self.prepare_field(field, poses)
+            self._run("forward", lambda: N.library().dpt_b200_forward(self.problem, self.rays(poses), packed.data_ptr(),
+                                             out.data_ptr(), self.status.data_ptr(),
+                                             _stream(self.device)))
+            if checked:
+                self.consume_status()
+            return out
+
+    def vjp(self, field: torch.Tensor, poses: torch.Tensor, cotangent: torch.Tensor, *,
+            volume: bool, pose: Literal["matrix", "tangent", None] = "matrix",
+            volume_dtype: torch.dtype = torch.float32, checked: bool = True,
+            ) -> tuple[torch.Tensor | None, torch.Tensor | None]:
+        """Volume gradient (voxels, ``volume_dtype``) and per-view pose gradient
+        (``(views, 12)`` packed or ``(views, 6)`` local-right tangent)."""
+        if not volume and pose is None:
+            raise ContractError("request at least one projection gradient")
+        with self.lock, torch.cuda.device(self.device):
+            lib = N.library()
+            field = self.check_field(field)
+            poses = self.check_poses(poses)
+            cot = self._cotangent(cotangent)
+            packed = self.prepare_field(field, poses)
+            flags = N.VJP_VOLUME if volume else 0
+            components = 0
+            if pose == "matrix":
+                flags |= N.VJP_POSE12
+                components = 12
+            elif pose == "tangent":
+                flags |= N.VJP_POSE6
+                components = 6
+            accumulator = self.accumulator().data_ptr() if volume else None
+            partials = self.partials() if components else None
+            gradient = (torch.empty(self.plan.grid.shape, dtype=volume_dtype, device=self.device)
+                        if volume else None)
+            grad_code = N.F64 if volume_dtype == torch.float64 else N.F32
+            stream = _stream(self.device)
+            batch = self.spec.batch_views if volume else self.views
+            rays_per_view = self.plan.rays_per_view
+            element = cot.element_size()
+            for first in range(0, self.views, batch):
+                count = min(batch, self.views - first)
+                seed_ptr = cot.data_ptr() + first * rays_per_view * element
+                part_ptr = None
+                if partials is not None:
+                    tiles = lib.dpt_b200_pose_partials_bytes(self.problem, 1) // (12 * 8)
+                    part_ptr = partials.data_ptr() + first * tiles * components * 8
+                self._run("vjp", lambda: lib.dpt_b200_vjp(self.problem, self.rays(poses, first, count), packed.data_ptr(),
+                                     seed_ptr, flags, accumulator, part_ptr, self.status.data_ptr(),
+                                     stream), first, count)
+                if volume:
+                    last = first + count >= self.views
+                    single = count >= self.views
+                    self._run("fold", lambda: lib.dpt_b200_fold_volume(
+                            self.problem, accumulator,
+                            None if single else self.total().data_ptr(),
+                            1 if first > 0 else 0,
+                            gradient.data_ptr() if last else None, grad_code, 1,
+                            self.status.data_ptr(), stream))
+            pose_gradient = None
+            if components:
+                pose_gradient = torch.empty((self.views, components), dtype=torch.float64,
+                                            device=self.device)
+                self._run("finish_pose", lambda: lib.dpt_b200_finish_pose(self.problem, 0, self.views, components,
+                                             partials.data_ptr(), pose_gradient.data_ptr(), 0,
+                                             self.status.data_ptr(), stream))
+            if checked:
+                self.consume_status()
+            return gradient, pose_gradient
+
+    def pose_sensitivities(self, field: torch.Tensor, poses: torch.Tensor, cotangent: torch.Tensor,
+                           *, checked: bool = True) -> torch.Tensor:
+        """Per-ray rows ``cotangent[p] * dL[p]/d xi`` in local-right order, shape (rays, 6)."""
+        with self.lock, torch.cuda.device(self.device):
+            field = self.check_field(field)
+            poses = self.check_poses(poses)
+            cot = self._cotangent(cotangent)
+            packed = self.prepare_field(field, poses)
+            out = torch.empty((self.plan.rays, 6), dtype=torch.float64, device=self.device)
+            self._run("pose_sensitivities", lambda: N.library().dpt_b200_vjp(self.problem, self.rays(poses), packed.data_ptr(),
+                                         cot.data_ptr(), N.VJP_PER_RAY6, None, out.data_ptr(),
+                                         self.status.data_ptr(), _stream(self.device)))
+            if checked:
+                self.consume_status()
+            return out
+
+    def counts(self, poses: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        """Per-ray clip interval (lower, upper) and realised midpoint count."""
+        with self.lock, torch.cuda.device(self.device):
+            poses = self.check_poses(poses)
+            n = self.plan.rays
+            lower = torch.empty(n, dtype=torch.float64, device=self.device)
+            upper = torch.empty(n, dtype=torch.float64, device=self.device)
+            realised = torch.empty(n, dtype=torch.int32, device=self.device)
+            self._run("counts", lambda: N.library().dpt_b200_counts(self.problem, self.rays(poses), lower.data_ptr(),
+                                            upper.data_ptr(), realised.data_ptr(),
+                                            self.status.data_ptr(), _stream(self.device)))
+            return lower, upper, realised
+
+    # ------------------------------------------------------------ helpers
+    def _cotangent(self, cotangent: torch.Tensor) -> torch.Tensor:
+        if not isinstance(cotangent, torch.Tensor) or cotangent.device != self.device:
+            raise ContractError("cotangent must be a Torch tensor on the workspace device")
+        if cotangent.dtype != self.spec.image_dtype or cotangent.numel() != self.plan.rays:
+            raise ContractError("cotangent must match the projected image shape and dtype")
+        flat = cotangent.contiguous().reshape(-1)
+        if flat.stride() != (1,):
+            flat = flat.clone()
+        return flat
+
+
+def prepare_projection(grid: GridSpec, geometry, spec: ProjectionSpec, *,
+                       device: str | torch.device = "cuda:0") -> ProjectionWorkspace:
+    """Build the plan of ``grid`` and ``geometry`` and its device workspace."""
+    if not isinstance(spec, ProjectionSpec):
+        raise ContractError("spec must be a ProjectionSpec")
+    return ProjectionWorkspace(plan_rays(grid, geometry), spec, device)
+
+
+def project_optical_depth(field: torch.Tensor, pose: torch.Tensor, *, workspace: ProjectionWorkspace,
+                          out_L: torch.Tensor | None = None) -> torch.Tensor:
+    """``L[p] = integral mu(r_p(s)) ds`` for every ray of the workspace."""
+    return workspace.forward(field, pose, out_L)
+
+
+def projection_vjp(field: torch.Tensor, pose: torch.Tensor, *, cotangent: torch.Tensor,
+                   workspace: ProjectionWorkspace, pose_gradient: Literal["matrix", "tangent", None] = "tangent",
+                   volume_gradient: bool = True,
+                   volume_gradient_precision: Literal["float32", "float64"] = "float32"):
+    """``(grad_mu, grad_pose) = J^T cotangent`` of the projection."""
+    dtype = torch.float64 if volume_gradient_precision == "float64" else torch.float32
+    return workspace.vjp(field, pose, cotangent, volume=volume_gradient, pose=pose_gradient,
+                         volume_dtype=dtype)
+
+
+def projection_pose_sensitivities(field: torch.Tensor, pose: torch.Tensor, *, cotangent: torch.Tensor,
+                                  workspace: ProjectionWorkspace) -> torch.Tensor:
+    """Per-ray weighted local-right pose Jacobian rows, shape (rays, 6)."""
+    return workspace.pose_sensitivities(field, pose, cotangent)

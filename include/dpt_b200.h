@@ -1,0 +1,201 @@
+/*
+ * dpt_b200.h - C ABI of the B200 differentiable CT projector.
+ *
+ * The projector integrates a sampled attenuation field mu (mm^-1) along finite
+ * source-to-detector segments: clipped midpoint sampling of the trilinear,
+ * half-cell-extended field, then L = |e - s| * step * sum_i mu(p_i).  Its VJP
+ * returns the volume cotangent (adjoint backprojection) and the per-view rigid
+ * pose cotangent.
+ *
+ * Every compute entry point borrows caller memory and allocates nothing: the
+ * field, geometry, outputs and scratch are device pointers owned by the
+ * caller, work is enqueued on the caller's cudaStream_t (passed as void*), and
+ * the call returns as soon as the kernels are enqueued.  Device diagnostics are
+ * OR-ed into per-view int32 status words with the reference projector's bits:
+ *   1 = invalid rigid pose, 2 = non-finite projection / gradient / cotangent,
+ *   8 = field not finite or negative.
+ * Host-side argument errors are returned as negative DPT_E* codes; a CUDA launch
+ * error is returned as its positive cudaError_t value.
+ *
+ * The reference interfaces these entry points replace (hcltech-robotics/dpt):
+ *   dpt_b200_prepare_field  <- python/dpt/torch/_projection_ops.py:197-211 (_validate:
+ *                              field scan + rigid-pose check) and the field upload of
+ *                              python/dpt/projection.py:747-809
+ *   dpt_b200_forward        <- python/dpt/projection.py:747-809 (project_optical_depth),
+ *                              kernels python/dpt/kernels/projection_fp32.py:334-374 and
+ *                              python/dpt/kernels/projection.py:802-846
+ *   dpt_b200_vjp            <- python/dpt/projection.py:871-1018 (projection_vjp) and
+ *                              1021-1084 (projection_pose_sensitivities), kernels
+ *                              python/dpt/kernels/projection_fp32.py:377-617 and
+ *                              python/dpt/kernels/projection.py:873-1237
+ *   dpt_b200_fold_volume    <- python/dpt/torch/_projection_ops.py:304-352 (FP64 widening
+ *                              of the FP32 volume gradient) plus the gradient finite scan
+ *                              python/dpt/projection.py:470-499
+ *   dpt_b200_finish_pose    <- python/dpt/_reductions.py:27-63 (FP64 tile tree and finish)
+ *   dpt_b200_counts         <- per-ray clip interval of python/dpt/kernels/projection_fp32.py:78-109
+ *                              and python/dpt/kernels/projection.py:147-184 (no separate
+ *                              reference entry point; exported for bit-exact count checks)
+ */
+#ifndef DPT_B200_H
+#define DPT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPT_B200_ABI_VERSION 1
+
+/* Storage / output element types. */
+enum {
+    DPT_F32 = 0,
+    DPT_F64 = 1,
+    DPT_F16 = 2,
+    DPT_BF16 = 3
+};
+
+/* Sample-loop arithmetic.
+ *  DPT_ARITH_F32   FP64 ray setup, FP32 clip, FP32 fmaf interpolation and serial FP32 ray sum
+ *                  (the reference "fp32" Projector, kernels/projection_fp32.py).
+ *  DPT_ARITH_F64   FP64 ray setup, clip, interpolation and sum (the reference "fp64" Projector,
+ *                  kernels/projection.py strict midpoint).
+ *  DPT_ARITH_F32C  FP64 ray setup and clip, FP32 marching and interpolation, compensated
+ *                  (Kahan) FP32 ray sum; the precision form for FP16/BF16 (and FP32) storage. */
+enum {
+    DPT_ARITH_F32 = 0,
+    DPT_ARITH_F64 = 1,
+    DPT_ARITH_F32C = 2
+};
+
+/* How rays are described. */
+enum {
+    DPT_RAYS_PANELS = 0, /* per-view panel table (cone, parallel or curved), row-major pixels */
+    DPT_RAYS_BUNDLE = 1  /* explicit FP64 source/endpoint arrays, one pose per view */
+};
+
+/* Panel table: DPT_VIEW_WORDS doubles per view. */
+#define DPT_VIEW_WORDS 20
+enum {
+    DPT_PANEL_CONE = 0,     /* words 0-2 source, 3-5 first pixel centre, 6-8 u*du, 9-11 v*dv */
+    DPT_PANEL_PARALLEL = 1, /* words 0-2 unit direction, 3-5 first pixel centre, 6-8 u, 9-11 v,
+                               12 du, 13 dv, 14 segment length */
+    DPT_PANEL_CURVED = 2    /* words 0-2 source, 3-5 first pixel centre, 6-8 u, 9-11 v,
+                               12 du, 13 dv, 14 radius, 15-17 radial vector */
+};
+#define DPT_VIEW_MODE_WORD 18
+
+/* Field layouts read by the sampling kernels.
+ *  DPT_LAYOUT_REPLICATED  corner-replicated copy written by dpt_b200_prepare_field (default):
+ *                         FP32 storage 16 bytes per voxel, FP16/BF16 storage 16 bytes per voxel.
+ *  DPT_LAYOUT_DIRECT      eight gathers per sample straight from the caller's FP32 field;
+ *                         `packed` then points at the field itself (no copy, FP32 only). */
+enum {
+    DPT_LAYOUT_REPLICATED = 0,
+    DPT_LAYOUT_DIRECT = 1
+};
+
+/* VJP flags. */
+enum {
+    DPT_VJP_VOLUME = 1,      /* scatter the volume cotangent into the accumulator */
+    DPT_VJP_POSE12 = 2,      /* per-view packed 12-entry pose cotangent (row-major R, t) */
+    DPT_VJP_POSE6 = 4,       /* per-view local-right tangent (tx,ty,tz,rx,ry,rz) */
+    DPT_VJP_PER_RAY6 = 8     /* per-ray local-right 6-row Jacobian (weighted by the cotangent) */
+};
+
+/* Error codes (negative). */
+enum {
+    DPT_OK = 0,
+    DPT_E_NULL = -1,       /* a required pointer is null */
+    DPT_E_SHAPE = -2,      /* a size is out of range */
+    DPT_E_DTYPE = -3,      /* unsupported dtype / arithmetic combination */
+    DPT_E_FLAGS = -4,      /* inconsistent flags */
+    DPT_E_RANGE = -5,      /* view range outside the problem */
+    DPT_E_ALIGN = -6,      /* a pointer is not aligned as required */
+    DPT_E_CAPACITY = -7    /* a fixed-capacity buffer is too small */
+};
+
+/* Fixed description of one projection problem. */
+typedef struct dpt_problem {
+    int32_t nx, ny, nz;     /* grid sample counts; field is x fastest: (z*ny + y)*nx + x */
+    int32_t views;          /* number of views */
+    int32_t rows, cols;     /* detector shape per view; bundles use rows=1, cols=rays per view */
+    int32_t samples;        /* midpoint samples per ray */
+    int32_t ray_kind;       /* DPT_RAYS_* */
+    int32_t arith;          /* DPT_ARITH_* */
+    int32_t field_dtype;    /* DPT_F32, DPT_F16 or DPT_BF16 */
+    int32_t image_dtype;    /* DPT_F32 or DPT_F64: image and cotangent element type */
+    int32_t layout;         /* DPT_LAYOUT_*: how the sampling kernels read the field */
+    double object_to_grid[9]; /* diag(1/h) G^T, row-major: grid index = M (x_object - origin) */
+    double grid_origin[3];    /* object mm of sample (0,0,0) */
+} dpt_problem;
+
+/* Ray description for one call.  All pointers are device pointers. */
+typedef struct dpt_rays {
+    const double* poses;        /* views x 12, row-major object-to-world R then t (mm) */
+    const double* view_table;   /* views x DPT_VIEW_WORDS, for DPT_RAYS_PANELS */
+    const double* ray_sources;  /* views*rows*cols x 3, for DPT_RAYS_BUNDLE */
+    const double* ray_endpoints;/* views*rows*cols x 3, for DPT_RAYS_BUNDLE */
+    int32_t view_begin;         /* first view of this call */
+    int32_t view_count;         /* number of views of this call */
+} dpt_rays;
+
+/* Library identity. */
+int dpt_b200_abi_version(void);
+const char* dpt_b200_error_string(int code);
+
+/* Scratch sizes in bytes (all 256-byte aligned allocations are sufficient). */
+size_t dpt_b200_packed_bytes(const dpt_problem* problem);
+size_t dpt_b200_accumulator_bytes(const dpt_problem* problem);
+size_t dpt_b200_pose_partials_bytes(const dpt_problem* problem, int32_t view_count);
+
+/* Validate the field (bit 8 into status[0]) and every view's rigid pose (bit 1 into
+ * status[view]); write the corner-replicated copy of the field used by the sampling
+ * kernels into `packed` (dpt_b200_packed_bytes, 16-byte aligned).  A null `packed`
+ * only validates (an unchanged field whose copy is still current). */
+int dpt_b200_prepare_field(const dpt_problem* problem, const void* field, void* packed,
+                           const double* poses, int32_t* status, void* stream);
+
+/* Optical depth of views [view_begin, view_begin+view_count): `image` holds
+ * view_count*rows*cols elements of image_dtype in view, row, column order. */
+int dpt_b200_forward(const dpt_problem* problem, const dpt_rays* rays, const void* packed,
+                     void* image, int32_t* status, void* stream);
+
+/* Discrete VJP of the same views.  `cotangent` matches `image` of dpt_b200_forward.
+ * DPT_VJP_VOLUME adds into `accumulator` (dpt_b200_accumulator_bytes, zeroed by the caller
+ * before its first use).  A pose flag writes per-block FP64 partials into `pose_partials`
+ * (dpt_b200_pose_partials_bytes); dpt_b200_finish_pose turns them into gradients.
+ * DPT_VJP_PER_RAY6 writes 6 doubles per ray into `pose_partials` instead. */
+int dpt_b200_vjp(const dpt_problem* problem, const dpt_rays* rays, const void* packed,
+                 const void* cotangent, int32_t flags, float* accumulator,
+                 double* pose_partials, int32_t* status, void* stream);
+
+/* Reduce the pose partials of a dpt_b200_vjp call over views [view_begin, view_begin +
+ * view_count) in a fixed FP64 order into `pose_gradient` (view_count x components,
+ * components 12 or 6); accumulate != 0 adds.  Non-finite results set bit 2 of
+ * status[view]. */
+int dpt_b200_finish_pose(const dpt_problem* problem, int32_t view_begin, int32_t view_count,
+                         int32_t components,
+                         const double* pose_partials, double* pose_gradient, int32_t accumulate,
+                         int32_t* status, void* stream);
+
+/* Fold the corner accumulator into per-voxel sums.  `total` (voxels doubles, may be null)
+ * receives total (+)= fold in FP64.  When `gradient` is non-null the final FP32
+ * (gradient_dtype DPT_F32) or FP64 gradient is written from total (or from the fold when
+ * total is null) and scanned for non-finite values (bit 2 into status[0]).  The accumulator
+ * is cleared for the next batch when clear != 0. */
+int dpt_b200_fold_volume(const dpt_problem* problem, float* accumulator, double* total,
+                         int32_t accumulate_total, void* gradient, int32_t gradient_dtype,
+                         int32_t clear, int32_t* status, void* stream);
+
+/* Per-ray clip interval (the arithmetic's own lower/upper, as doubles) and the number of
+ * midpoint samples that fall inside the half-cell support. */
+int dpt_b200_counts(const dpt_problem* problem, const dpt_rays* rays, double* lower,
+                    double* upper, int32_t* realised, int32_t* status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DPT_B200_H */

@@ -1,0 +1,1173 @@
+/*
+ * projector_oracle.c - CPU ORACLE for the projector.  TEST INFRASTRUCTURE ONLY.
+ *
+ * This file restates, scalar and unoptimised, the arithmetic of the reference
+ * projector (hcltech-robotics/dpt) so that the CUDA kernels can be checked
+ * against it.  It is called only by tests/, by __graft_entry__.smoke() and by
+ * bench.py's CPU-baseline arm; the product never links or calls it.
+ *
+ * Reference files restated (paths inside the reference project):
+ *   python/dpt/kernels/projection.py       ray_for_pixel 79-102, valid_ray 110-121,
+ *                                          inside_support 124-134, finite_interval 147-184,
+ *                                          cell_lower/cell_fraction/corner_index 199-222,
+ *                                          sample_cell_fraction 236-274, midpoint forward
+ *                                          770-846, strict VJP 873-1237
+ *   python/dpt/kernels/projection_fp32.py  FP32 clip 78-109, sample_position/point 116-127,
+ *                                          coordinates 130-140, sample_field 157-177,
+ *                                          sample_pose_field 180-209, scatter_increment
+ *                                          240-258, cell-run aggregation 261-331 and
+ *                                          459-548, forward 334-374, VJP 377-617
+ *   python/dpt/kernels/geometry.py         unpack 13-21, local-right adjoint 24-52,
+ *                                          rigid-pose check 55-74
+ *   python/dpt/kernels/batched_geometry.py generate 8-39 (parallel / curved panels)
+ *   python/dpt/kernels/projection_checks.py field/finite scans 20-28
+ *
+ * Floating-point contract.  Compile with -ffp-contract=off: every fused
+ * multiply-add below is an explicit fma()/fmaf(), every other operation is a
+ * single IEEE-rounded operation.  Where the reference writes a*b + c*d (which
+ * its JIT may contract) this restatement uses fma(c, d, a*b); where it writes
+ * a + b*c it uses fma(b, c, a).  The CUDA kernels follow the same contract, so
+ * forward images, clip intervals and sample counts agree bit for bit.
+ *
+ * The DPT_ARITH_F32C form (FP64 clip, FP32 marching, compensated sum) has no
+ * reference counterpart: it is the storage-precision form of this build and is
+ * checked here against its own definition and, in the tests, against F64.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../include/dpt_b200.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ storage */
+
+static float half_to_float(uint16_t h)
+{
+    uint32_t sign = (uint32_t)(h >> 15) << 31;
+    uint32_t exponent = (h >> 10) & 0x1f;
+    uint32_t mantissa = h & 0x3ff;
+    uint32_t bits;
+    if (exponent == 0) {
+        if (mantissa == 0) {
+            bits = sign;
+        } else {
+            /* subnormal half: value = mantissa * 2^-24, exact in float */
+            float value = (float)mantissa * 5.9604644775390625e-08f;
+            memcpy(&bits, &value, 4);
+            bits |= sign;
+        }
+    } else if (exponent == 31) {
+        bits = sign | 0x7f800000u | (mantissa << 13);
+    } else {
+        bits = sign | ((exponent + 112) << 23) | (mantissa << 13);
+    }
+    float out;
+    memcpy(&out, &bits, 4);
+    return out;
+}
+
+static float bf16_to_float(uint16_t b)
+{
+    uint32_t bits = (uint32_t)b << 16;
+    float out;
+    memcpy(&out, &bits, 4);
+    return out;
+}
+
+static float field_value(const dpt_problem* p, const void* field, int64_t index)
+{
+    switch (p->field_dtype) {
+    case DPT_F16:
+        return half_to_float(((const uint16_t*)field)[index]);
+    case DPT_BF16:
+        return bf16_to_float(((const uint16_t*)field)[index]);
+    default:
+        return ((const float*)field)[index];
+    }
+}
+
+/* --------------------------------------------------------------- ray setup */
+
+typedef struct {
+    double origin[3], direction[3];           /* grid-index coordinates */
+    double object_source[3], object_direction[3];
+    double world_source_relative[3], world_direction[3];
+    double length;
+} ray64_t;
+
+/* r = A v for a row-major 3x3 A, accumulated as fma(a2,v2, fma(a1,v1, a0*v0)). */
+static void matvec(const double* a, const double* v, double* r)
+{
+    for (int i = 0; i < 3; ++i)
+        r[i] = fma(a[3 * i + 2], v[2], fma(a[3 * i + 1], v[1], a[3 * i] * v[0]));
+}
+
+/* r = A^T v. */
+static void matvec_t(const double* a, const double* v, double* r)
+{
+    for (int i = 0; i < 3; ++i)
+        r[i] = fma(a[6 + i], v[2], fma(a[3 + i], v[1], a[i] * v[0]));
+}
+
+/* Source and endpoint of ray `pixel` (index inside its view).  Cone panels follow
+ * kernels/projection.py:88-93 (end = d0 + c*(u du) + r*(v dv)); parallel and
+ * curved panels follow kernels/batched_geometry.py:17-38. */
+static void ray_endpoints(const dpt_problem* p, const double* view_table, const double* sources,
+                          const double* endpoints, int view, int64_t pixel, double* source,
+                          double* end)
+{
+    if (p->ray_kind == DPT_RAYS_BUNDLE) {
+        int64_t ray = (int64_t)view * p->rows * p->cols + pixel;
+        for (int a = 0; a < 3; ++a) {
+            source[a] = sources[3 * ray + a];
+            end[a] = endpoints[3 * ray + a];
+        }
+        return;
+    }
+    const double* w = view_table + (int64_t)view * DPT_VIEW_WORDS;
+    double row = (double)(pixel / p->cols), column = (double)(pixel % p->cols);
+    int mode = (int)w[DPT_VIEW_MODE_WORD];
+    if (mode == DPT_PANEL_CONE) {
+        for (int a = 0; a < 3; ++a) {
+            source[a] = w[a];
+            end[a] = fma(row, w[9 + a], fma(column, w[6 + a], w[3 + a]));
+        }
+        return;
+    }
+    double du = w[12], dv = w[13], length = w[14];
+    if (mode == DPT_PANEL_PARALLEL) {
+        double cu = column * du, rv = row * dv;
+        for (int a = 0; a < 3; ++a) {
+            end[a] = fma(rv, w[9 + a], fma(cu, w[6 + a], w[3 + a]));
+            source[a] = end[a] - length * w[a];
+        }
+        return;
+    }
+    /* curved: angle = c*du/R; end = o + (cos-1) radial + sin R u + r dv v */
+    double angle = column * du / length;
+    double c1 = cos(angle) - 1.0, s = sin(angle) * length, rv = row * dv;
+    for (int a = 0; a < 3; ++a) {
+        source[a] = w[a];
+        end[a] = fma(rv, w[9 + a], fma(s, w[6 + a], fma(c1, w[15 + a], w[3 + a])));
+    }
+}
+
+/* kernels/projection.py:79-102 */
+static void ray_setup(const dpt_problem* p, const double* pose, const double* source,
+                      const double* end, ray64_t* r)
+{
+    double rel[3];
+    for (int a = 0; a < 3; ++a) {
+        r->world_source_relative[a] = source[a] - pose[9 + a];
+        r->world_direction[a] = end[a] - source[a];
+    }
+    matvec_t(pose, r->world_source_relative, r->object_source);
+    matvec_t(pose, r->world_direction, r->object_direction);
+    for (int a = 0; a < 3; ++a)
+        rel[a] = r->object_source[a] - p->grid_origin[a];
+    matvec(p->object_to_grid, rel, r->origin);
+    matvec(p->object_to_grid, r->object_direction, r->direction);
+    const double* d = r->world_direction;
+    r->length = sqrt(fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0])));
+}
+
+static int finite3(const double* v) { return isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]); }
+static int finite3f(const float* v) { return isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]); }
+
+/* kernels/projection.py:110-121 */
+static int valid_ray(const ray64_t* r)
+{
+    return finite3(r->origin) && finite3(r->direction) && finite3(r->object_source) &&
+           finite3(r->object_direction) && finite3(r->world_source_relative) &&
+           finite3(r->world_direction) && isfinite(r->length) && r->length > 0.0;
+}
+
+/* ----------------------------------------------------------------- clipping */
+
+typedef struct {
+    float lower, upper;
+    float lower_origin[3], lower_direction[3], upper_origin[3], upper_direction[3];
+} interval32_t;
+
+typedef struct {
+    double lower, upper;
+    double lower_origin[3], lower_direction[3], upper_origin[3], upper_direction[3];
+} interval64_t;
+
+/* kernels/projection_fp32.py:78-109 */
+static void clip32(const float* origin, const float* direction, const int* shape,
+                   interval32_t* iv)
+{
+    memset(iv, 0, sizeof(*iv));
+    iv->lower = 0.0f;
+    iv->upper = 1.0f;
+    for (int a = 0; a < 3; ++a) {
+        float low = -0.5f, high = (float)shape[a] - 0.5f, velocity = direction[a];
+        if (velocity == 0.0f) {
+            if (origin[a] < low || origin[a] > high)
+                iv->upper = -1.0f;
+        } else {
+            float first = (low - origin[a]) / velocity;
+            float last = (high - origin[a]) / velocity;
+            if (first > last) {
+                float t = first;
+                first = last;
+                last = t;
+            }
+            if (first > iv->lower) {
+                iv->lower = first;
+                memset(iv->lower_origin, 0, sizeof(iv->lower_origin));
+                memset(iv->lower_direction, 0, sizeof(iv->lower_direction));
+                iv->lower_origin[a] = -1.0f / velocity;
+                iv->lower_direction[a] = -first / velocity;
+            }
+            if (last < iv->upper) {
+                iv->upper = last;
+                memset(iv->upper_origin, 0, sizeof(iv->upper_origin));
+                memset(iv->upper_direction, 0, sizeof(iv->upper_direction));
+                iv->upper_origin[a] = -1.0f / velocity;
+                iv->upper_direction[a] = -last / velocity;
+            }
+        }
+    }
+}
+
+/* kernels/projection.py:147-184 */
+static void clip64(const double* origin, const double* direction, const int* shape,
+                   interval64_t* iv)
+{
+    memset(iv, 0, sizeof(*iv));
+    iv->lower = 0.0;
+    iv->upper = 1.0;
+    for (int a = 0; a < 3; ++a) {
+        double low = -0.5, high = (double)shape[a] - 0.5, velocity = direction[a];
+        if (velocity == 0.0) {
+            if (origin[a] < low || origin[a] > high)
+                iv->upper = -1.0;
+        } else {
+            double first = (low - origin[a]) / velocity;
+            double last = (high - origin[a]) / velocity;
+            if (first > last) {
+                double t = first;
+                first = last;
+                last = t;
+            }
+            if (first > iv->lower) {
+                iv->lower = first;
+                memset(iv->lower_origin, 0, sizeof(iv->lower_origin));
+                memset(iv->lower_direction, 0, sizeof(iv->lower_direction));
+                iv->lower_origin[a] = -1.0 / velocity;
+                iv->lower_direction[a] = -first / velocity;
+            }
+            if (last < iv->upper) {
+                iv->upper = last;
+                memset(iv->upper_origin, 0, sizeof(iv->upper_origin));
+                memset(iv->upper_direction, 0, sizeof(iv->upper_direction));
+                iv->upper_origin[a] = -1.0 / velocity;
+                iv->upper_direction[a] = -last / velocity;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------ interpolation */
+
+static int inside32(const float* q, const int* shape)
+{
+    return finite3f(q) && q[0] >= -0.5f && q[1] >= -0.5f && q[2] >= -0.5f &&
+           q[0] <= (float)shape[0] - 0.5f && q[1] <= (float)shape[1] - 0.5f &&
+           q[2] <= (float)shape[2] - 0.5f;
+}
+
+static int inside64(const double* q, const int* shape)
+{
+    return finite3(q) && q[0] >= -0.5 && q[1] >= -0.5 && q[2] >= -0.5 &&
+           q[0] <= (double)shape[0] - 0.5 && q[1] <= (double)shape[1] - 0.5 &&
+           q[2] <= (double)shape[2] - 0.5;
+}
+
+static int64_t corner_index(const int* lower, const int* shape, int corner)
+{
+    int x = lower[0] + (corner & 1), y = lower[1] + ((corner >> 1) & 1),
+        z = lower[2] + ((corner >> 2) & 1);
+    if (x > shape[0] - 1) x = shape[0] - 1;
+    if (y > shape[1] - 1) y = shape[1] - 1;
+    if (z > shape[2] - 1) z = shape[2] - 1;
+    return ((int64_t)z * shape[1] + y) * shape[0] + x;
+}
+
+static int cell_floor(double value, int n)
+{
+    int lower = (int)floor(value), cap = n - 2 > 0 ? n - 2 : 0;
+    return lower < cap ? lower : cap;
+}
+
+/* kernels/projection_fp32.py:130-140: lower cell, fraction and in-range slope mask. */
+static void coordinates32(const float* q, const int* shape, int* lower, float* fraction,
+                          float* slope)
+{
+    for (int a = 0; a < 3; ++a) {
+        float high = (float)(shape[a] - 1);
+        float value = q[a] < 0.0f ? 0.0f : (q[a] > high ? high : q[a]);
+        lower[a] = cell_floor((double)value, shape[a]);
+        fraction[a] = value - (float)lower[a];
+        slope[a] = (q[a] >= 0.0f && q[a] < high) ? 1.0f : 0.0f;
+    }
+}
+
+/* kernels/projection.py:199-214 */
+static void coordinates64(const double* q, const int* shape, int* lower, double* fraction,
+                          double* slope)
+{
+    for (int a = 0; a < 3; ++a) {
+        double high = (double)(shape[a] - 1);
+        double value = q[a] < 0.0 ? 0.0 : (q[a] > high ? high : q[a]);
+        lower[a] = cell_floor(value, shape[a]);
+        fraction[a] = value - (double)lower[a];
+        slope[a] = (q[a] >= 0.0 && q[a] < high) ? 1.0 : 0.0;
+    }
+}
+
+/* (f0 f1) f2 with f = 1 - fraction for a 0 bit, kernels/projection_fp32.py:143-154 */
+static float corner_weight32(const float* fraction, int corner)
+{
+    float f[3];
+    for (int a = 0; a < 3; ++a)
+        f[a] = ((corner >> a) & 1) ? fraction[a] : 1.0f - fraction[a];
+    return (f[0] * f[1]) * f[2];
+}
+
+/* sample_pose_field, kernels/projection_fp32.py:180-209 (value and grid slope). */
+static float sample32(const dpt_problem* p, const void* field, const float* q, const int* shape,
+                      float* gradient)
+{
+    if (gradient) gradient[0] = gradient[1] = gradient[2] = 0.0f;
+    if (!inside32(q, shape)) return 0.0f;
+    int lower[3];
+    float fraction[3], slope[3], v[8];
+    coordinates32(q, shape, lower, fraction, slope);
+    float value = 0.0f;
+    for (int c = 0; c < 8; ++c) {
+        v[c] = field_value(p, field, corner_index(lower, shape, c));
+        value = fmaf(corner_weight32(fraction, c), v[c], value);
+    }
+    if (gradient) {
+        float fx = fraction[0], fy = fraction[1], fz = fraction[2];
+        float ax = 1.0f - fx, ay = 1.0f - fy, az = 1.0f - fz;
+        float x0 = fmaf(fy, v[3] - v[2], ay * (v[1] - v[0]));
+        float x1 = fmaf(fy, v[7] - v[6], ay * (v[5] - v[4]));
+        gradient[0] = slope[0] * fmaf(fz, x1, az * x0);
+        float y0 = fmaf(fx, v[3] - v[1], ax * (v[2] - v[0]));
+        float y1 = fmaf(fx, v[7] - v[5], ax * (v[6] - v[4]));
+        gradient[1] = slope[1] * fmaf(fz, y1, az * y0);
+        float z0 = fmaf(fx, v[5] - v[1], ax * (v[4] - v[0]));
+        float z1 = fmaf(fx, v[7] - v[3], ax * (v[6] - v[2]));
+        gradient[2] = slope[2] * fmaf(fy, z1, ay * z0);
+    }
+    return value;
+}
+
+/* sample_cell_fraction, kernels/projection.py:236-274 (weighted lerps in FP64). */
+static double sample64(const dpt_problem* p, const void* field, const double* q,
+                       const int* shape, double* gradient)
+{
+    if (gradient) gradient[0] = gradient[1] = gradient[2] = 0.0;
+    if (!inside64(q, shape)) return 0.0;
+    int lower[3];
+    double f[3], slope[3], v[8];
+    coordinates64(q, shape, lower, f, slope);
+    for (int c = 0; c < 8; ++c)
+        v[c] = (double)field_value(p, field, corner_index(lower, shape, c));
+    double fx = f[0], fy = f[1], fz = f[2], ax = 1.0 - fx, ay = 1.0 - fy, az = 1.0 - fz;
+    double x00 = fma(fx, v[1], ax * v[0]), x10 = fma(fx, v[3], ax * v[2]);
+    double x01 = fma(fx, v[5], ax * v[4]), x11 = fma(fx, v[7], ax * v[6]);
+    double xy0 = fma(fy, x10, ay * x00), xy1 = fma(fy, x11, ay * x01);
+    double value = fma(fz, xy1, az * xy0);
+    if (gradient) {
+        double dx00 = v[1] - v[0], dx10 = v[3] - v[2], dx01 = v[5] - v[4], dx11 = v[7] - v[6];
+        double dx0 = fma(fy, dx10, ay * dx00), dx1 = fma(fy, dx11, ay * dx01);
+        double dy0 = fma(fx, v[3] - v[1], ax * (v[2] - v[0]));
+        double dy1 = fma(fx, v[7] - v[5], ax * (v[6] - v[4]));
+        double dz0 = fma(fx, v[5] - v[1], ax * (v[4] - v[0]));
+        double dz1 = fma(fx, v[7] - v[3], ax * (v[6] - v[2]));
+        gradient[0] = slope[0] * fma(fz, dx1, az * dx0);
+        gradient[1] = slope[1] * fma(fz, dy1, az * dy0);
+        gradient[2] = slope[2] * fma(fy, dz1, ay * dz0);
+    }
+    return value;
+}
+
+/* ------------------------------------------------------------ ray geometry */
+
+typedef struct {
+    /* common per-ray quantities, FP64 setup plus the arithmetic's own clip */
+    ray64_t r;
+    int valid;
+    /* F32 */
+    float o32[3], d32[3], len32;
+    interval32_t iv32;
+    /* F64 and F32C */
+    interval64_t iv64;
+} ray_t;
+
+static int ray_prepare(const dpt_problem* p, const double* pose, const double* source,
+                       const double* end, ray_t* ray)
+{
+    int shape[3] = {p->nx, p->ny, p->nz};
+    ray_setup(p, pose, source, end, &ray->r);
+    ray->valid = valid_ray(&ray->r);
+    if (p->arith == DPT_ARITH_F32) {
+        for (int a = 0; a < 3; ++a) {
+            ray->o32[a] = (float)ray->r.origin[a];
+            ray->d32[a] = (float)ray->r.direction[a];
+        }
+        ray->len32 = (float)ray->r.length;
+        ray->valid = ray->valid && finite3f(ray->o32) && finite3f(ray->d32) &&
+                     isfinite(ray->len32) && ray->len32 > 0.0f;
+        if (ray->valid) clip32(ray->o32, ray->d32, shape, &ray->iv32);
+    } else if (ray->valid) {
+        clip64(ray->r.origin, ray->r.direction, shape, &ray->iv64);
+    }
+    return ray->valid;
+}
+
+/* F32C marching: entry = o + lower d and per-sample step vector, both rounded once to FP32
+ * (the mixed-midpoint recurrence of kernels/projection.py:368-392). */
+static void march32c(const ray_t* ray, int samples, float* entry, float* step_vector)
+{
+    double span = ray->iv64.upper - ray->iv64.lower, step = span / (double)samples;
+    for (int a = 0; a < 3; ++a) {
+        entry[a] = (float)fma(ray->iv64.lower, ray->r.direction[a], ray->r.origin[a]);
+        step_vector[a] = (float)(step * ray->r.direction[a]);
+    }
+}
+
+static void point32c(const float* entry, const float* step_vector, int index, float* q)
+{
+    float offset = (float)index + 0.5f;
+    for (int a = 0; a < 3; ++a)
+        q[a] = fmaf(offset, step_vector[a], entry[a]);
+}
+
+/* ------------------------------------------------------------------ forward */
+
+/* One ray's optical depth; returns status bits. */
+static int forward_ray(const dpt_problem* p, const void* field, const ray_t* ray, double* out)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0, S = p->samples;
+    *out = 0.0;
+    if (!ray->valid) return 2;
+    if (p->arith == DPT_ARITH_F32) {
+        /* kernels/projection_fp32.py:359-372 */
+        const interval32_t* iv = &ray->iv32;
+        float total = 0.0f;
+        if (iv->upper > iv->lower) {
+            float step = (iv->upper - iv->lower) / (float)S;
+            for (int i = 0; i < S; ++i) {
+                float position = fmaf((float)i + 0.5f, step, iv->lower), q[3];
+                for (int a = 0; a < 3; ++a) q[a] = fmaf(position, ray->d32[a], ray->o32[a]);
+                if (!finite3f(q)) status |= 2;
+                total += sample32(p, field, q, shape, NULL);
+            }
+            total *= ray->len32 * step;
+        }
+        if (!isfinite(total)) status |= 2;
+        *out = total;
+    } else if (p->arith == DPT_ARITH_F64) {
+        /* kernels/projection.py:826-844 with get_midpoint_integrator 770-799 */
+        const interval64_t* iv = &ray->iv64;
+        double integral = 0.0;
+        if (iv->upper > iv->lower) {
+            double step = (iv->upper - iv->lower) / (double)S;
+            for (int i = 0; i < S; ++i) {
+                double position = fma((double)i + 0.5, step, iv->lower), q[3];
+                for (int a = 0; a < 3; ++a) q[a] = fma(position, ray->r.direction[a], ray->r.origin[a]);
+                if (!finite3(q)) status |= 2;
+                integral += sample64(p, field, q, shape, NULL);
+            }
+            integral *= ray->r.length * step;
+        }
+        *out = integral;
+        if (!isfinite(p->image_dtype == DPT_F32 ? (double)(float)integral : integral)) status |= 2;
+    } else {
+        /* F32C: FP32 samples with a compensated sum, FP64 scale. */
+        const interval64_t* iv = &ray->iv64;
+        double integral = 0.0;
+        if (iv->upper > iv->lower) {
+            float entry[3], stepv[3], sum = 0.0f, carry = 0.0f;
+            march32c(ray, S, entry, stepv);
+            for (int i = 0; i < S; ++i) {
+                float q[3];
+                point32c(entry, stepv, i, q);
+                if (!finite3f(q)) status |= 2;
+                float y = sample32(p, field, q, shape, NULL) - carry;
+                float t = sum + y;
+                carry = (t - sum) - y;
+                sum = t;
+            }
+            double step = (iv->upper - iv->lower) / (double)S;
+            integral = ((double)sum - (double)carry) * (ray->r.length * step);
+        }
+        *out = integral;
+        if (!isfinite(p->image_dtype == DPT_F32 ? (double)(float)integral : integral)) status |= 2;
+    }
+    return status;
+}
+
+static void store_image(const dpt_problem* p, void* image, int64_t index, double value)
+{
+    if (p->image_dtype == DPT_F64)
+        ((double*)image)[index] = value;
+    else
+        ((float*)image)[index] = (float)value;
+}
+
+static double load_image(const dpt_problem* p, const void* image, int64_t index)
+{
+    if (p->image_dtype == DPT_F64) return ((const double*)image)[index];
+    return (double)((const float*)image)[index];
+}
+
+int oracle_forward(const dpt_problem* p, const double* poses, const double* view_table,
+                   const double* sources, const double* endpoints, const void* field,
+                   void* image, int32_t* status, int threads)
+{
+    int64_t per_view = (int64_t)p->rows * p->cols, total = per_view * p->views;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int64_t ray_index = 0; ray_index < total; ++ray_index) {
+        int view = (int)(ray_index / per_view);
+        int64_t pixel = ray_index % per_view;
+        double source[3], end[3], out;
+        ray_t ray;
+        ray_endpoints(p, view_table, sources, endpoints, view, pixel, source, end);
+        ray_prepare(p, poses + 12 * view, source, end, &ray);
+        int bits = forward_ray(p, field, &ray, &out);
+        store_image(p, image, ray_index, out);
+        if (bits) {
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+            status[view] |= bits;
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ counts */
+
+int oracle_counts(const dpt_problem* p, const double* poses, const double* view_table,
+                  const double* sources, const double* endpoints, double* lower, double* upper,
+                  int32_t* realised, int threads)
+{
+    int shape[3] = {p->nx, p->ny, p->nz};
+    int64_t per_view = (int64_t)p->rows * p->cols, total = per_view * p->views;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int64_t ray_index = 0; ray_index < total; ++ray_index) {
+        int view = (int)(ray_index / per_view);
+        double source[3], end[3];
+        ray_t ray;
+        ray_endpoints(p, view_table, sources, endpoints, view, ray_index % per_view, source, end);
+        ray_prepare(p, poses + 12 * view, source, end, &ray);
+        int count = 0;
+        double lo = 0.0, hi = -1.0;
+        if (ray.valid && p->arith == DPT_ARITH_F32) {
+            lo = ray.iv32.lower;
+            hi = ray.iv32.upper;
+            if (ray.iv32.upper > ray.iv32.lower) {
+                float step = (ray.iv32.upper - ray.iv32.lower) / (float)p->samples;
+                for (int i = 0; i < p->samples; ++i) {
+                    float position = fmaf((float)i + 0.5f, step, ray.iv32.lower), q[3];
+                    for (int a = 0; a < 3; ++a) q[a] = fmaf(position, ray.d32[a], ray.o32[a]);
+                    count += inside32(q, shape);
+                }
+            }
+        } else if (ray.valid && p->arith == DPT_ARITH_F64) {
+            lo = ray.iv64.lower;
+            hi = ray.iv64.upper;
+            if (hi > lo) {
+                double step = (hi - lo) / (double)p->samples;
+                for (int i = 0; i < p->samples; ++i) {
+                    double position = fma((double)i + 0.5, step, lo), q[3];
+                    for (int a = 0; a < 3; ++a) q[a] = fma(position, ray.r.direction[a], ray.r.origin[a]);
+                    count += inside64(q, shape);
+                }
+            }
+        } else if (ray.valid) {
+            lo = ray.iv64.lower;
+            hi = ray.iv64.upper;
+            if (hi > lo) {
+                float entry[3], stepv[3];
+                march32c(&ray, p->samples, entry, stepv);
+                for (int i = 0; i < p->samples; ++i) {
+                    float q[3];
+                    point32c(entry, stepv, i, q);
+                    count += inside32(q, shape);
+                }
+            }
+        }
+        lower[ray_index] = lo;
+        upper[ray_index] = hi;
+        realised[ray_index] = count;
+    }
+    return 0;
+}
+
+/* --------------------------------------------------------------------- VJP */
+
+/* scatter_increment, kernels/projection_fp32.py:240-258: one rounded product, then the
+ * flush of |x| < 2^-126 to signed zero that CUDA global FP32 atomics apply. */
+static float scatter_increment(float factor, float weight)
+{
+    float increment = factor * weight;
+    if (fabsf(increment) < 0x1p-126f) return copysignf(0.0f, increment);
+    return increment;
+}
+
+typedef struct {
+    double* gradient; /* private FP64 volume accumulator */
+    int shape[3];
+    int pending[3];
+    float sums[8];
+    int carry; /* shared-face carry (volume-only VJP), kernels/projection_fp32.py:396 */
+} scatter_t;
+
+static void flush_all(scatter_t* s)
+{
+    for (int c = 0; c < 8; ++c) {
+        s->gradient[corner_index(s->pending, s->shape, c)] += (double)s->sums[c];
+        s->sums[c] = 0.0f;
+    }
+}
+
+/* transition_cell, kernels/projection_fp32.py:272-331 */
+static void transition(scatter_t* s, const int* next)
+{
+    int* lo = s->pending;
+    if (s->shape[0] > 1 && s->shape[1] > 1 && s->shape[2] > 1) {
+        int d[3] = {next[0] - lo[0], next[1] - lo[1], next[2] - lo[2]};
+        for (int axis = 0; axis < 3; ++axis) {
+            int o1 = (axis + 1) % 3, o2 = (axis + 2) % 3;
+            if (d[o1] == 0 && d[o2] == 0 && (d[axis] == 1 || d[axis] == -1)) {
+                int shared_bit = d[axis] == 1 ? 1 : 0;
+                float carried[8] = {0};
+                for (int c = 0; c < 8; ++c) {
+                    if (((c >> axis) & 1) == shared_bit)
+                        carried[c ^ (1 << axis)] = s->sums[c];
+                    else
+                        s->gradient[corner_index(lo, s->shape, c)] += (double)s->sums[c];
+                }
+                memcpy(s->sums, carried, sizeof(carried));
+                return;
+            }
+        }
+    }
+    flush_all(s);
+}
+
+/* One ray of the FP32 joint VJP, kernels/projection_fp32.py:411-602. */
+static int vjp_ray_f32(const dpt_problem* p, const void* field, const ray_t* ray, float seed,
+                       int flags, scatter_t* sc, double* g12, double* g6)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0, S = p->samples;
+    int active_volume = (flags & DPT_VJP_VOLUME) != 0;
+    int active_pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
+    const interval32_t* iv = &ray->iv32;
+    float span = iv->upper - iv->lower;
+    if (!isfinite(seed)) status |= 2;
+    if (!(span > 0.0f && seed != 0.0f)) return status;
+    float step = span / (float)S;
+    float physical_step = ray->len32 * step;
+    float volume_factor = seed * physical_step;
+    float mean = 0.0f, direct_origin[3] = {0}, direct_direction[3] = {0};
+    float shift_lower = 0.0f, shift_upper = 0.0f;
+    int bounded = isfinite(volume_factor) && fabsf(volume_factor) <= 1.0f;
+    sc->pending[0] = sc->pending[1] = sc->pending[2] = -1;
+    memset(sc->sums, 0, sizeof(sc->sums));
+    for (int i = 0; i < S; ++i) {
+        float position = fmaf((float)i + 0.5f, step, iv->lower), q[3];
+        for (int a = 0; a < 3; ++a) q[a] = fmaf(position, ray->d32[a], ray->o32[a]);
+        if (!finite3f(q)) status |= 2;
+        if (active_pose) {
+            float g[3];
+            float value = sample32(p, field, q, shape, g);
+            mean += value;
+            for (int a = 0; a < 3; ++a) {
+                direct_origin[a] += g[a];
+                direct_direction[a] = fmaf(position, g[a], direct_direction[a]);
+            }
+            float alpha = ((float)i + 0.5f) / (float)S;
+            float along = fmaf(g[2], ray->d32[2], fmaf(g[1], ray->d32[1], g[0] * ray->d32[0]));
+            shift_lower = fmaf(1.0f - alpha, along, shift_lower);
+            shift_upper = fmaf(alpha, along, shift_upper);
+        }
+        if (active_volume) {
+            if (inside32(q, shape)) {
+                int lower[3];
+                float fraction[3], slope[3];
+                coordinates32(q, shape, lower, fraction, slope);
+                if (lower[0] != sc->pending[0] || lower[1] != sc->pending[1] ||
+                    lower[2] != sc->pending[2]) {
+                    if (sc->pending[0] >= 0) {
+                        if (sc->carry && bounded)
+                            transition(sc, lower);
+                        else
+                            flush_all(sc);
+                    } else {
+                        memset(sc->sums, 0, sizeof(sc->sums));
+                    }
+                    memcpy(sc->pending, lower, sizeof(lower));
+                }
+                for (int c = 0; c < 8; ++c) {
+                    float increment = scatter_increment(volume_factor, corner_weight32(fraction, c));
+                    if (bounded) {
+                        sc->sums[c] += increment;
+                    } else if (!isfinite(increment)) {
+                        status |= 2;
+                        sc->gradient[corner_index(lower, shape, c)] += (double)increment;
+                    } else {
+                        float partial = sc->sums[c] + increment;
+                        if (!isfinite(partial)) {
+                            sc->gradient[corner_index(lower, shape, c)] += (double)sc->sums[c];
+                            sc->sums[c] = increment;
+                        } else {
+                            sc->sums[c] = partial;
+                        }
+                    }
+                }
+            } else if (sc->pending[0] >= 0) {
+                flush_all(sc);
+                sc->pending[0] = sc->pending[1] = sc->pending[2] = -1;
+            }
+        }
+    }
+    if (active_volume && sc->pending[0] >= 0) flush_all(sc);
+    if (!active_pose) return status;
+
+    /* kernels/projection_fp32.py:549-602 */
+    float lower_seed = fmaf(span, shift_lower, -mean);
+    float upper_seed = fmaf(span, shift_upper, mean);
+    float og[3], dg[3];
+    for (int a = 0; a < 3; ++a) {
+        og[a] = fmaf(upper_seed, iv->upper_origin[a],
+                     fmaf(lower_seed, iv->lower_origin[a], span * direct_origin[a]));
+        dg[a] = fmaf(upper_seed, iv->upper_direction[a],
+                     fmaf(lower_seed, iv->lower_direction[a], span * direct_direction[a]));
+    }
+    float factor = (seed * ray->len32) / (float)S;
+    double og64[3] = {og[0], og[1], og[2]}, dg64[3] = {dg[0], dg[1], dg[2]};
+    double sa[3], da[3];
+    matvec_t(p->object_to_grid, og64, sa);
+    matvec_t(p->object_to_grid, dg64, da);
+    for (int a = 0; a < 3; ++a) {
+        sa[a] = (double)factor * sa[a];
+        da[a] = (double)factor * da[a];
+    }
+    if (g12) {
+        const double* wsr = ray->r.world_source_relative;
+        const double* wd = ray->r.world_direction;
+        for (int row = 0; row < 3; ++row)
+            for (int col = 0; col < 3; ++col)
+                g12[3 * row + col] = fma(wd[row], da[col], wsr[row] * sa[col]);
+        /* translation = -(R sa); R is the pose rotation, supplied through g12[12..20] */
+    }
+    if (g6) {
+        /* local-right adjoint, kernels/geometry.py:24-52 */
+        const double* os = ray->r.object_source;
+        const double* od = ray->r.object_direction;
+        g6[0] = -sa[0];
+        g6[1] = -sa[1];
+        g6[2] = -sa[2];
+        g6[3] = fma(-da[2], od[1], da[1] * od[2]) + fma(-sa[2], os[1], sa[1] * os[2]);
+        g6[4] = fma(-da[0], od[2], da[2] * od[0]) + fma(-sa[0], os[2], sa[2] * os[0]);
+        g6[5] = fma(-da[1], od[0], da[0] * od[1]) + fma(-sa[1], os[0], sa[0] * os[1]);
+    }
+    /* store the source adjoint for the translation rows */
+    if (g12) {
+        g12[12] = sa[0];
+        g12[13] = sa[1];
+        g12[14] = sa[2];
+    }
+    return status;
+}
+
+/* One ray of the strict FP64 joint VJP (midpoint), kernels/projection.py:922-1217, with
+ * FP32-rounded volume increments (scatter_realised, kernels/projection.py:407-430). */
+static int vjp_ray_f64(const dpt_problem* p, const void* field, const ray_t* ray, double seed,
+                       int flags, scatter_t* sc, double* g12, double* g6)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0, S = p->samples;
+    int active_volume = (flags & DPT_VJP_VOLUME) != 0;
+    int active_pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
+    const interval64_t* iv = &ray->iv64;
+    double span = iv->upper - iv->lower;
+    if (!isfinite(seed)) status |= 2;
+    if (seed == 0.0) span = 0.0;
+    if (!(span > 0.0)) return status;
+    double factor = seed * ray->r.length;
+    double step = span / (double)S;
+    double volume_factor = factor * span / (double)S;
+    int power_of_two = S > 0 && (S & (S - 1)) == 0;
+    double inverse_samples = power_of_two ? 1.0 / (double)S : 0.0;
+    double mean = 0.0, direct_origin[3] = {0}, direct_direction[3] = {0};
+    double shift_lower = 0.0, shift_upper = 0.0;
+    for (int i = 0; i < S; ++i) {
+        double alpha = power_of_two ? ((double)i + 0.5) * inverse_samples
+                                    : ((double)i + 0.5) / (double)S;
+        double position = fma((double)i + 0.5, step, iv->lower), q[3];
+        for (int a = 0; a < 3; ++a) q[a] = fma(position, ray->r.direction[a], ray->r.origin[a]);
+        if (!finite3(q)) status |= 2;
+        int supported = inside64(q, shape);
+        if (active_pose) {
+            double g[3];
+            double value = sample64(p, field, q, shape, g);
+            mean += value;
+            for (int a = 0; a < 3; ++a) {
+                direct_origin[a] += g[a];
+                direct_direction[a] = fma(position, g[a], direct_direction[a]);
+            }
+            const double* d = ray->r.direction;
+            double along = fma(g[2], d[2], fma(g[1], d[1], g[0] * d[0]));
+            shift_lower = fma(1.0 - alpha, along, shift_lower);
+            shift_upper = fma(alpha, along, shift_upper);
+        }
+        if (active_volume && supported) {
+            int lower[3];
+            double fraction[3], slope[3];
+            coordinates64(q, shape, lower, fraction, slope);
+            for (int c = 0; c < 8; ++c) {
+                double contribution = volume_factor;
+                for (int a = 0; a < 3; ++a)
+                    contribution *= ((c >> a) & 1) ? fraction[a] : 1.0 - fraction[a];
+                float rounded = (float)contribution;
+                if (!isfinite(rounded)) status |= 2;
+                sc->gradient[corner_index(lower, shape, c)] += (double)rounded;
+            }
+        }
+    }
+    if (!active_pose) return status;
+    double lower_seed = fma(span, shift_lower, -mean);
+    double upper_seed = fma(span, shift_upper, mean);
+    double og[3], dg[3];
+    for (int a = 0; a < 3; ++a) {
+        og[a] = fma(upper_seed, iv->upper_origin[a],
+                    fma(lower_seed, iv->lower_origin[a], span * direct_origin[a]));
+        dg[a] = fma(upper_seed, iv->upper_direction[a],
+                    fma(lower_seed, iv->lower_direction[a], span * direct_direction[a]));
+    }
+    factor /= (double)S;
+    double sa[3], da[3];
+    matvec_t(p->object_to_grid, og, sa);
+    matvec_t(p->object_to_grid, dg, da);
+    for (int a = 0; a < 3; ++a) {
+        sa[a] = factor * sa[a];
+        da[a] = factor * da[a];
+    }
+    if (g12) {
+        const double* wsr = ray->r.world_source_relative;
+        const double* wd = ray->r.world_direction;
+        for (int row = 0; row < 3; ++row)
+            for (int col = 0; col < 3; ++col)
+                g12[3 * row + col] = fma(wd[row], da[col], wsr[row] * sa[col]);
+        g12[12] = sa[0];
+        g12[13] = sa[1];
+        g12[14] = sa[2];
+    }
+    if (g6) {
+        const double* os = ray->r.object_source;
+        const double* od = ray->r.object_direction;
+        g6[0] = -sa[0];
+        g6[1] = -sa[1];
+        g6[2] = -sa[2];
+        g6[3] = fma(-da[2], od[1], da[1] * od[2]) + fma(-sa[2], os[1], sa[1] * os[2]);
+        g6[4] = fma(-da[0], od[2], da[2] * od[0]) + fma(-sa[0], os[2], sa[2] * os[0]);
+        g6[5] = fma(-da[1], od[0], da[0] * od[1]) + fma(-sa[1], os[0], sa[0] * os[1]);
+    }
+    return status;
+}
+
+/* One ray of the F32C VJP: FP64 clip and clip-face chain, FP32 marching and sample
+ * arithmetic, pose moments G = sum grad, H = sum alpha grad and the integral sum. */
+static int vjp_ray_f32c(const dpt_problem* p, const void* field, const ray_t* ray, double seed,
+                        int flags, scatter_t* sc, double* g12, double* g6)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0, S = p->samples;
+    int active_volume = (flags & DPT_VJP_VOLUME) != 0;
+    int active_pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
+    const interval64_t* iv = &ray->iv64;
+    double span = iv->upper - iv->lower;
+    if (!isfinite(seed)) status |= 2;
+    if (!(span > 0.0 && seed != 0.0)) return status;
+    double step = span / (double)S;
+    float volume_factor = (float)(seed * ray->r.length * step);
+    int bounded = isfinite(volume_factor) && fabsf(volume_factor) <= 1.0f;
+    float entry[3], stepv[3];
+    march32c(ray, S, entry, stepv);
+    float mean = 0.0f, mean_carry = 0.0f, G[3] = {0}, H[3] = {0};
+    float inv_s = 1.0f / (float)S;
+    sc->pending[0] = sc->pending[1] = sc->pending[2] = -1;
+    memset(sc->sums, 0, sizeof(sc->sums));
+    for (int i = 0; i < S; ++i) {
+        float q[3];
+        point32c(entry, stepv, i, q);
+        if (!finite3f(q)) status |= 2;
+        if (active_pose) {
+            float g[3];
+            float value = sample32(p, field, q, shape, g);
+            float y = value - mean_carry, t = mean + y;
+            mean_carry = (t - mean) - y;
+            mean = t;
+            float alpha = ((float)i + 0.5f) * inv_s;
+            for (int a = 0; a < 3; ++a) {
+                G[a] += g[a];
+                H[a] = fmaf(alpha, g[a], H[a]);
+            }
+        }
+        if (active_volume) {
+            if (inside32(q, shape)) {
+                int lower[3];
+                float fraction[3], slope[3];
+                coordinates32(q, shape, lower, fraction, slope);
+                if (lower[0] != sc->pending[0] || lower[1] != sc->pending[1] ||
+                    lower[2] != sc->pending[2]) {
+                    if (sc->pending[0] >= 0) flush_all(sc);
+                    memset(sc->sums, 0, sizeof(sc->sums));
+                    memcpy(sc->pending, lower, sizeof(lower));
+                }
+                for (int c = 0; c < 8; ++c) {
+                    float increment = scatter_increment(volume_factor, corner_weight32(fraction, c));
+                    if (bounded) {
+                        sc->sums[c] += increment;
+                    } else {
+                        if (!isfinite(increment)) status |= 2;
+                        sc->gradient[corner_index(lower, shape, c)] += (double)increment;
+                    }
+                }
+            } else if (sc->pending[0] >= 0) {
+                flush_all(sc);
+                sc->pending[0] = sc->pending[1] = sc->pending[2] = -1;
+            }
+        }
+    }
+    if (active_volume && sc->pending[0] >= 0) flush_all(sc);
+    if (!active_pose) return status;
+    const double* d = ray->r.direction;
+    double Gd[3] = {G[0], G[1], G[2]}, Hd[3] = {H[0], H[1], H[2]};
+    double mean64 = (double)mean - (double)mean_carry;
+    double g_along = fma(Gd[2], d[2], fma(Gd[1], d[1], Gd[0] * d[0]));
+    double h_along = fma(Hd[2], d[2], fma(Hd[1], d[1], Hd[0] * d[0]));
+    double shift_upper = h_along, shift_lower = g_along - h_along;
+    double lower_seed = fma(span, shift_lower, -mean64);
+    double upper_seed = fma(span, shift_upper, mean64);
+    double og[3], dg[3];
+    for (int a = 0; a < 3; ++a) {
+        double direct_direction = fma(span, Hd[a], iv->lower * Gd[a]);
+        og[a] = fma(upper_seed, iv->upper_origin[a],
+                    fma(lower_seed, iv->lower_origin[a], span * Gd[a]));
+        dg[a] = fma(upper_seed, iv->upper_direction[a],
+                    fma(lower_seed, iv->lower_direction[a], span * direct_direction));
+    }
+    double factor = seed * ray->r.length / (double)S;
+    double sa[3], da[3];
+    matvec_t(p->object_to_grid, og, sa);
+    matvec_t(p->object_to_grid, dg, da);
+    for (int a = 0; a < 3; ++a) {
+        sa[a] = factor * sa[a];
+        da[a] = factor * da[a];
+    }
+    if (g12) {
+        const double* wsr = ray->r.world_source_relative;
+        const double* wd = ray->r.world_direction;
+        for (int row = 0; row < 3; ++row)
+            for (int col = 0; col < 3; ++col)
+                g12[3 * row + col] = fma(wd[row], da[col], wsr[row] * sa[col]);
+        g12[12] = sa[0];
+        g12[13] = sa[1];
+        g12[14] = sa[2];
+    }
+    if (g6) {
+        const double* os = ray->r.object_source;
+        const double* od = ray->r.object_direction;
+        g6[0] = -sa[0];
+        g6[1] = -sa[1];
+        g6[2] = -sa[2];
+        g6[3] = fma(-da[2], od[1], da[1] * od[2]) + fma(-sa[2], os[1], sa[1] * os[2]);
+        g6[4] = fma(-da[0], od[2], da[2] * od[0]) + fma(-sa[0], os[2], sa[2] * os[0]);
+        g6[5] = fma(-da[1], od[0], da[0] * od[1]) + fma(-sa[1], os[0], sa[0] * os[1]);
+    }
+    return status;
+}
+
+/*
+ * Joint VJP over all rays.
+ *   volume_gradient: voxels doubles, accumulated (+=) in FP64 when DPT_VJP_VOLUME.
+ *   pose_gradient:   DPT_VJP_POSE12 -> views x 12, DPT_VJP_POSE6 -> views x 6,
+ *                    DPT_VJP_PER_RAY6 -> rays x 6 (overwritten).
+ * Per-view pose sums run over rays in order, in FP64.
+ */
+int oracle_vjp(const dpt_problem* p, const double* poses, const double* view_table,
+               const double* sources, const double* endpoints, const void* field,
+               const void* cotangent, int32_t flags, double* volume_gradient,
+               double* pose_gradient, int32_t* status, int threads)
+{
+    int64_t per_view = (int64_t)p->rows * p->cols, total = per_view * p->views;
+    int64_t voxels = (int64_t)p->nx * p->ny * p->nz;
+    int components = (flags & DPT_VJP_POSE12) ? 12 : 6;
+    int want_pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
+    int nthreads = 1;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+    nthreads = omp_get_max_threads();
+#endif
+    /* Per-thread private volume accumulators; bounded to keep host memory modest. */
+    int64_t limit_threads = (int64_t)(16ll << 30) / (voxels * 8 > 0 ? voxels * 8 : 1);
+    if (limit_threads < 1) limit_threads = 1;
+    if (nthreads > limit_threads) nthreads = (int)limit_threads;
+    double** privates = NULL;
+    if (flags & DPT_VJP_VOLUME) {
+        privates = (double**)calloc((size_t)nthreads, sizeof(double*));
+        for (int t = 0; t < nthreads; ++t) {
+            privates[t] = (double*)calloc((size_t)voxels, sizeof(double));
+            if (!privates[t]) return -1;
+        }
+    }
+    double* per_ray = NULL;
+    if (want_pose) {
+        per_ray = (double*)calloc((size_t)total * 15 + 1, sizeof(double));
+        if (!per_ray) return -1;
+    }
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nthreads)
+#endif
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        scatter_t sc;
+        memset(&sc, 0, sizeof(sc));
+        sc.shape[0] = p->nx;
+        sc.shape[1] = p->ny;
+        sc.shape[2] = p->nz;
+        sc.gradient = privates ? privates[tid] : NULL;
+        sc.carry = (flags & DPT_VJP_VOLUME) && !want_pose;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+        for (int64_t ray_index = 0; ray_index < total; ++ray_index) {
+            int view = (int)(ray_index / per_view);
+            double source[3], end[3], g12[15] = {0}, g6[6] = {0};
+            ray_t ray;
+            ray_endpoints(p, view_table, sources, endpoints, view, ray_index % per_view, source, end);
+            ray_prepare(p, poses + 12 * view, source, end, &ray);
+            double seed = load_image(p, cotangent, ray_index);
+            int bits = 0;
+            if (!ray.valid) {
+                bits = 2;
+            } else if (p->arith == DPT_ARITH_F32) {
+                bits = vjp_ray_f32(p, field, &ray, (float)seed, flags, &sc,
+                                   (flags & DPT_VJP_POSE12) ? g12 : NULL,
+                                   (flags & (DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) ? g6 : NULL);
+            } else if (p->arith == DPT_ARITH_F64) {
+                bits = vjp_ray_f64(p, field, &ray, seed, flags, &sc,
+                                   (flags & DPT_VJP_POSE12) ? g12 : NULL,
+                                   (flags & (DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) ? g6 : NULL);
+            } else {
+                bits = vjp_ray_f32c(p, field, &ray, seed, flags, &sc,
+                                    (flags & DPT_VJP_POSE12) ? g12 : NULL,
+                                    (flags & (DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) ? g6 : NULL);
+            }
+            if (want_pose) {
+                double* slot = per_ray + 15 * ray_index;
+                if (flags & DPT_VJP_POSE12) {
+                    /* translation rows -(R sa), kernels/projection_fp32.py:591-593 */
+                    const double* R = poses + 12 * view;
+                    double t[3];
+                    matvec(R, g12 + 12, t);
+                    for (int k = 0; k < 9; ++k) slot[k] = g12[k];
+                    for (int a = 0; a < 3; ++a) slot[9 + a] = -t[a];
+                } else {
+                    for (int k = 0; k < 6; ++k) slot[k] = g6[k];
+                }
+                if (flags & DPT_VJP_PER_RAY6)
+                    for (int k = 0; k < 6; ++k)
+                        if (!isfinite(slot[k])) bits |= 2;
+            }
+            if (bits) {
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+                status[view] |= bits;
+            }
+        }
+    }
+    if (privates) {
+        for (int64_t v = 0; v < voxels; ++v) {
+            double sum = 0.0;
+            for (int t = 0; t < nthreads; ++t) sum += privates[t][v];
+            volume_gradient[v] += sum;
+        }
+        for (int t = 0; t < nthreads; ++t) free(privates[t]);
+        free(privates);
+    }
+    if (want_pose) {
+        if (flags & DPT_VJP_PER_RAY6) {
+            for (int64_t r = 0; r < total; ++r)
+                for (int k = 0; k < 6; ++k) pose_gradient[6 * r + k] = per_ray[15 * r + k];
+        } else {
+            for (int view = 0; view < p->views; ++view) {
+                for (int k = 0; k < components; ++k) {
+                    double sum = 0.0;
+                    for (int64_t px = 0; px < per_view; ++px)
+                        sum += per_ray[15 * ((int64_t)view * per_view + px) + k];
+                    pose_gradient[components * view + k] = sum;
+                    if (!isfinite(sum)) status[view] |= 2;
+                }
+            }
+        }
+        free(per_ray);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------- checks */
+
+/* kernels/projection_checks.py:20-24 (physical field: finite and non-negative) */
+int oracle_check_field(const dpt_problem* p, const void* field, int64_t voxels)
+{
+    for (int64_t v = 0; v < voxels; ++v) {
+        float value = field_value(p, field, v);
+        if (!isfinite(value) || value < 0.0f) return 8;
+    }
+    return 0;
+}
+
+/* kernels/geometry.py:55-74: finite, R^T R = I to 1e-10, det >= 0. */
+int oracle_check_pose(const double* pose)
+{
+    for (int k = 0; k < 12; ++k)
+        if (!isfinite(pose[k])) return 1;
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) {
+            double product = 0.0;
+            for (int k = 0; k < 3; ++k) product += pose[3 * k + i] * pose[3 * k + j];
+            if (fabs(product - (i == j ? 1.0 : 0.0)) > 1e-10) return 1;
+        }
+    }
+    const double* r = pose;
+    double det = r[0] * (r[4] * r[8] - r[5] * r[7]) - r[1] * (r[3] * r[8] - r[5] * r[6]) +
+                 r[2] * (r[3] * r[7] - r[4] * r[6]);
+    return det < 0.0 ? 1 : 0;
+}
+
+int oracle_abi_version(void) { return DPT_B200_ABI_VERSION; }

@@ -1,0 +1,164 @@
+"""CUDA kernels (through the C ABI) against the CPU oracle on the same seeded inputs.
+
+Bars: forward images, clip intervals and realised sample counts are bit-exact for
+the FP32 and FP64 arithmetic (same floating-point contract); FP32 volume
+gradients agree to 2e-5 relative L2 (atomic summation order), pose gradients to
+1e-9 relative (FP64 reduction order); the compensated form agrees to 1e-6.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from dpt_b200 import _native as N
+from dpt_b200.plan import plan_rays
+from dpt_b200.projection import ProjectionSpec, ProjectionWorkspace
+from oracle import oracle as O
+from scenes import cone_scene, fp32_fixture, identity_poses, mixed_panels, poses_for
+
+pytestmark = pytest.mark.gpu
+
+ARITH = {"float32": O.ARITH_F32, "float64": O.ARITH_F64, "compensated": O.ARITH_F32C}
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def workspace(grid, geometry, samples, sampling="float32", precision="float32", storage="float32",
+              layout="replicated", widen=None):
+    spec = ProjectionSpec(samples, precision=precision, sampling_precision=sampling,
+                          storage_precision=storage, layout=layout, widen_views=widen)
+    return ProjectionWorkspace(plan_rays(grid, geometry), spec, "cuda:0")
+
+
+def device_inputs(values, poses, dtype=torch.float32):
+    field = torch.tensor(np.asarray(values, dtype=np.float32), device="cuda:0").to(dtype).contiguous()
+    return field, torch.tensor(poses, dtype=torch.float64, device="cuda:0")
+
+
+@pytest.mark.parametrize("samples", [17, 97, 1024])
+def test_fp32_forward_bit_exact_on_reference_matrix_scene(samples):
+    grid, rays, data = fp32_fixture()
+    ws = workspace(grid, rays, samples)
+    field, pose = device_inputs(data["values"].reshape(grid.shape), data["pose"])
+    image = ws.forward(field, pose).cpu().numpy()
+    expected, status = O.forward(ws.plan, data["values"], data["pose"], samples=samples)
+    assert not status.any()
+    np.testing.assert_array_equal(image, expected)
+    # and within the reference test's tolerance of its own FP32 weight matrix
+    np.testing.assert_allclose(image, data[f"matrix_{samples}"] @ data["values"].astype(np.float64),
+                               rtol=2e-5, atol=3e-7)
+
+
+@pytest.mark.parametrize("sampling", ["float32", "float64", "compensated"])
+@pytest.mark.parametrize("layout", ["replicated", "direct"])
+def test_cone_forward_and_counts_bit_exact(sampling, layout):
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views))
+    precision = "float64" if sampling == "float64" else "float32"
+    ws = workspace(grid, geometry, 61, sampling, precision, layout=layout)
+    field, pose = device_inputs(values, poses)
+    image = ws.forward(field, pose).cpu().numpy().reshape(-1)
+    expected, status = O.forward(ws.plan, values, poses, samples=61, arith=ARITH[sampling],
+                                 image_dtype=O.F64 if precision == "float64" else O.F32)
+    assert not status.any()
+    np.testing.assert_array_equal(image, expected)
+    lower, upper, realised = (t.cpu().numpy() for t in ws.counts(pose))
+    e_lower, e_upper, e_realised = O.counts(ws.plan, poses, samples=61, arith=ARITH[sampling])
+    np.testing.assert_array_equal(lower, e_lower)
+    np.testing.assert_array_equal(upper, e_upper)
+    np.testing.assert_array_equal(realised, e_realised)
+    assert realised.sum() > 0
+
+
+def test_parallel_and_curved_panels_match_oracle():
+    grid, _, values = cone_scene()
+    geometry = mixed_panels(grid)
+    poses = poses_for(3, seed=4)
+    ws = workspace(grid, geometry, 45)
+    field, pose = device_inputs(values, poses)
+    image = ws.forward(field, pose).cpu().numpy().reshape(-1)
+    expected, _ = O.forward(ws.plan, values, poses, samples=45)
+    # curved panels use the device's sincos: compare with a tolerance there
+    np.testing.assert_array_equal(image[: 2 * 99], expected[: 2 * 99])
+    np.testing.assert_allclose(image[2 * 99:], expected[2 * 99:], rtol=1e-5, atol=1e-7)
+    assert np.abs(expected).sum() > 0
+
+
+@pytest.mark.parametrize("sampling", ["float32", "float64", "compensated"])
+@pytest.mark.parametrize("pose_form", ["matrix", "tangent"])
+def test_joint_vjp_matches_oracle(sampling, pose_form):
+    grid, geometry, values = cone_scene()
+    views = len(geometry.views)
+    poses = poses_for(views, seed=2)
+    precision = "float64" if sampling == "float64" else "float32"
+    ws = workspace(grid, geometry, 53, sampling, precision, widen=3)
+    field, pose = device_inputs(values, poses)
+    rng = np.random.default_rng(9)
+    seed = rng.uniform(-1.0, 1.0, ws.plan.rays).astype(np.float64 if precision == "float64" else np.float32)
+    cot = torch.tensor(seed, device="cuda:0").reshape(ws.plan.image_shape)
+    volume, pose_grad = ws.vjp(field, pose, cot, volume=True, pose=pose_form)
+    flags = O.VJP_VOLUME | (O.VJP_POSE12 if pose_form == "matrix" else O.VJP_POSE6)
+    e_volume, e_pose, status = O.vjp(ws.plan, values, poses, seed, samples=53, flags=flags,
+                                     arith=ARITH[sampling], image_dtype=O.F64 if precision == "float64" else O.F32)
+    assert not status.any()
+    assert rel_l2(volume.cpu().numpy().reshape(-1), e_volume) < 2e-6
+    np.testing.assert_allclose(pose_grad.cpu().numpy(), e_pose, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("storage", ["float16", "bfloat16"])
+def test_half_storage_forward_and_vjp_match_oracle(storage):
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views), seed=3)
+    ws = workspace(grid, geometry, 47, "compensated", storage=storage)
+    dtype = torch.float16 if storage == "float16" else torch.bfloat16
+    field, pose = device_inputs(values, poses, dtype)
+    half = field.cpu()
+    image = ws.forward(field, pose).cpu().numpy().reshape(-1)
+    code = O.F16 if storage == "float16" else O.BF16
+    raw = half.view(torch.int16).numpy().view(np.uint16)
+    expected, _ = O.forward(ws.plan, raw, poses, samples=47, arith=O.ARITH_F32C, field_dtype=code)
+    np.testing.assert_array_equal(image, expected)
+    seed = np.random.default_rng(1).uniform(0.1, 1.0, ws.plan.rays).astype(np.float32)
+    cot = torch.tensor(seed, device="cuda:0").reshape(ws.plan.image_shape)
+    volume, pose_grad = ws.vjp(field, pose, cot, volume=True, pose="tangent")
+    e_volume, e_pose, _ = O.vjp(ws.plan, raw, poses, seed, samples=47, flags=O.VJP_VOLUME | O.VJP_POSE6,
+                                arith=O.ARITH_F32C, field_dtype=code)
+    assert rel_l2(volume.cpu().numpy().reshape(-1), e_volume) < 2e-6
+    np.testing.assert_allclose(pose_grad.cpu().numpy(), e_pose, rtol=1e-9, atol=1e-12)
+
+
+def test_per_ray_pose_rows_sum_to_view_gradient():
+    grid, geometry, values = cone_scene(views=2)
+    poses = poses_for(2, seed=6)
+    ws = workspace(grid, geometry, 40)
+    field, pose = device_inputs(values, poses)
+    seed = np.random.default_rng(2).uniform(-1, 1, ws.plan.rays).astype(np.float32)
+    cot = torch.tensor(seed, device="cuda:0").reshape(ws.plan.image_shape)
+    rows = ws.pose_sensitivities(field, pose, cot).cpu().numpy()
+    _, tangent = ws.vjp(field, pose, cot, volume=False, pose="tangent")
+    per_view = rows.reshape(2, -1, 6).sum(axis=1)
+    np.testing.assert_allclose(per_view, tangent.cpu().numpy(), rtol=1e-10, atol=1e-13)
+    e_rows, _, _ = O.vjp(ws.plan, values, poses, seed, samples=40, flags=O.VJP_PER_RAY6)
+    np.testing.assert_array_equal(rows, e_rows)
+
+
+def test_identity_pose_bundle_single_voxel_known_answer():
+    """Clipped single-voxel case of the reference FP32 tests: L = 0.025*0.7."""
+    from dpt_b200.geometry import RayBundleGeometry
+    from dpt_b200.volumes import GridSpec
+
+    grid = GridSpec((1, 1, 1), (1.0, 1.0, 1.0))
+    rays = RayBundleGeometry(((-2.0, 0.0, 0.0),), ((0.2, 0.0, 0.0),))
+    ws = workspace(grid, rays, 1024)
+    field, pose = device_inputs(np.array([[[0.025]]], dtype=np.float32), identity_poses(1))
+    image = ws.forward(field, pose).cpu().numpy()
+    np.testing.assert_allclose(image, [0.025 * 0.7], rtol=2e-5)
+    cot = torch.ones(1, device="cuda:0")
+    volume, tangent = ws.vjp(field, pose, cot, volume=True, pose="tangent")
+    np.testing.assert_allclose(volume.cpu().numpy().reshape(-1), [0.7], rtol=2e-5)
+    np.testing.assert_allclose(tangent.cpu().numpy().reshape(-1), [-0.025, 0, 0, 0, 0, 0], rtol=2e-5, atol=1e-8)
