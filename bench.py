@@ -220,6 +220,7 @@ def run_gpu(args) -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=device)
 
+    from dpt_b200.distributed import reduce_volume_gradient
     from dpt_b200.torch import Projector
     from dpt_b200.torch import _projection_ops as ops
 
@@ -242,8 +243,7 @@ def run_gpu(args) -> None:
         residual = image - t
         loss = 0.5 * (residual.double() * residual.double()).sum()
         grad_field, grad_pose = torch.autograd.grad(loss, (f, xi))
-        if dist is not None:
-            dist.all_reduce(grad_field)
+        reduce_volume_gradient(grad_field)
         return loss.detach(), image.detach(), grad_field, grad_pose
 
     # realised ray-samples of one step (identity tangent: the poses of the timed steps)

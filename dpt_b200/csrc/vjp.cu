@@ -69,6 +69,21 @@ __device__ __forceinline__ void pose_rows(int mode, const Ray64& r, const double
     }
 }
 
+// Pose epilogue: recompute the FP64 ray of `pixel` (a few hundred FP64 operations once per
+// ray) instead of keeping its 24 registers alive across the sample loop, then form the rows.
+// The empty asm with a memory clobber makes the compiler reload the view record from shared
+// memory here, so the recomputation cannot be folded into the pre-loop ray setup.
+__device__ __forceinline__ void pose_epilogue(const RayArgs& a, const ViewShared& vs, int view, int pixel,
+                                           int mode, const double* sa, const double* da, double* g)
+{
+    asm volatile("" ::: "memory");
+    double source[3], end[3];
+    ray_endpoints(a, vs.table, view, pixel, source, end);
+    Ray64 r;
+    ray_setup(a.grid, vs.pose, source, end, r);
+    pose_rows(mode, r, vs.pose, sa, da, g);
+}
+
 template <int kArith, class Field, bool kVol, bool kPose, typename Seed>
 __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
                                                 int mode, float* __restrict__ acc,
@@ -223,7 +238,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                             sa[k] = factor * sa[k];
                             da[k] = factor * da[k];
                         }
-                        pose_rows(mode, r, vs.pose, sa, da, g);
+                        pose_epilogue(a, vs, view, pixel, mode, sa, da, g);
                     }
                 }
             }
@@ -354,7 +369,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                             sa[k] = factor * sa[k];
                             da[k] = factor * da[k];
                         }
-                        pose_rows(mode, r, vs.pose, sa, da, g);
+                        pose_epilogue(a, vs, view, pixel, mode, sa, da, g);
                     }
                 }
             }
@@ -484,7 +499,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                             sa[k] = factor * sa[k];
                             da[k] = factor * da[k];
                         }
-                        pose_rows(mode, r, vs.pose, sa, da, g);
+                        pose_epilogue(a, vs, view, pixel, mode, sa, da, g);
                     }
                 }
             }
