@@ -59,6 +59,7 @@ class Problem(ctypes.Structure):
         ("field_dtype", ctypes.c_int32),
         ("image_dtype", ctypes.c_int32),
         ("layout", ctypes.c_int32),
+        ("block_cols", ctypes.c_int32),
         ("object_to_grid", ctypes.c_double * 9),
         ("grid_origin", ctypes.c_double * 3),
     ]

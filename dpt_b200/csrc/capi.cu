@@ -6,6 +6,8 @@
 
 namespace dpt {
 
+int block_cols(const dpt_problem& p) { return p.block_cols == 0 ? kDefaultBlockCols : p.block_cols; }
+
 int tiles_per_view(const dpt_problem& p, int* tiles_x)
 {
     if (p.ray_kind == DPT_RAYS_BUNDLE) {
@@ -13,8 +15,9 @@ int tiles_per_view(const dpt_problem& p, int* tiles_x)
         *tiles_x = (int)((rays + kBlock - 1) / kBlock);
         return *tiles_x;
     }
-    *tiles_x = (p.cols + kTileCols - 1) / kTileCols;
-    const int tiles_y = (p.rows + kTileRows - 1) / kTileRows;
+    const int cols = block_cols(p), rows = kBlock / cols;
+    *tiles_x = (p.cols + cols - 1) / cols;
+    const int tiles_y = (p.rows + rows - 1) / rows;
     return *tiles_x * tiles_y;
 }
 
@@ -33,6 +36,9 @@ RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status)
     a.samples = p.samples;
     a.ray_kind = p.ray_kind;
     a.tiles_per_view = tiles_per_view(p, &a.tiles_x);
+    a.block_cols = block_cols(p);
+    a.block_rows = kBlock / a.block_cols;
+    a.warps_x = a.block_cols / 8;
     a.poses = r.poses;
     a.view_table = r.view_table;
     a.ray_sources = r.ray_sources;
@@ -70,6 +76,9 @@ int check_problem(const dpt_problem* p)
     if (p->field_dtype != DPT_F32 && p->arith != DPT_ARITH_F32C) return DPT_E_DTYPE;
     if (p->layout != DPT_LAYOUT_REPLICATED && p->layout != DPT_LAYOUT_DIRECT) return DPT_E_FLAGS;
     if (p->layout == DPT_LAYOUT_DIRECT && p->field_dtype != DPT_F32) return DPT_E_DTYPE;
+    if (p->block_cols != 0 && p->block_cols != 8 && p->block_cols != 16 && p->block_cols != 32 &&
+        p->block_cols != 64)
+        return DPT_E_FLAGS;
     // FP32 grid coordinates are exact integers only up to 2^24 (reference projection.py:548).
     if (p->arith != DPT_ARITH_F64 && (p->nx > (1 << 24) || p->ny > (1 << 24) || p->nz > (1 << 24)))
         return DPT_E_SHAPE;

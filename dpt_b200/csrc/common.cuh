@@ -19,8 +19,7 @@
 namespace dpt {
 
 constexpr int kBlock = 256;      // threads per block of the ray kernels
-constexpr int kTileCols = 16;    // detector columns per block tile
-constexpr int kTileRows = 16;    // detector rows per block tile
+constexpr int kDefaultBlockCols = 16;  // default block tile: 16 x 16 detector pixels
 
 struct Grid {
     int nx, ny, nz;
@@ -38,6 +37,9 @@ struct RayArgs {
     int ray_kind;
     int tiles_x;         // column tiles per view (panels)
     int tiles_per_view;  // blocks per view
+    int block_cols;      // detector columns per block tile (panels): 8, 16, 32 or 64
+    int block_rows;      // detector rows per block tile: 2048 / (8 * block_cols)
+    int warps_x;         // warps along the columns of a block tile: block_cols / 8
     const double* poses;       // absolute view indexing
     const double* view_table;  // absolute view indexing
     const double* ray_sources;
@@ -82,11 +84,12 @@ __device__ __forceinline__ bool ray_of_thread(const RayArgs& a, int tile, int* p
         *pixel = index;
         return index < a.rows * a.cols;
     }
-    // 16x16 block tile; each warp covers 8 columns x 4 rows.
+    // block tile of block_cols x block_rows pixels; each warp covers 8 columns x 4 rows.
     const int warp = t >> 5, lane = t & 31;
+    const int wy = warp / a.warps_x, wx = warp - wy * a.warps_x;
     const int tile_row = tile / a.tiles_x, tile_col = tile - tile_row * a.tiles_x;
-    const int col = tile_col * kTileCols + (warp & 1) * 8 + (lane & 7);
-    const int row = tile_row * kTileRows + (warp >> 1) * 4 + (lane >> 3);
+    const int col = tile_col * a.block_cols + wx * 8 + (lane & 7);
+    const int row = tile_row * a.block_rows + wy * 4 + (lane >> 3);
     *pixel = row * a.cols + col;
     return row < a.rows && col < a.cols;
 }

@@ -11,7 +11,8 @@ namespace dpt {
 // Fill a RayArgs record for views [view_begin, view_begin + view_count).
 RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status);
 
-// Blocks per view for the ray kernels.
+// Detector columns per block tile (panels) and blocks per view for the ray kernels.
+int block_cols(const dpt_problem& p);
 int tiles_per_view(const dpt_problem& p, int* tiles_x);
 
 cudaError_t launch_prepare_field(const dpt_problem& p, const void* field, void* packed,

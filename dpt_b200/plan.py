@@ -115,6 +115,7 @@ class RayPlan:
         field_dtype: int = N.F32,
         image_dtype: int = N.F32,
         layout: int = N.LAYOUT_REPLICATED,
+        block_cols: int = 0,
     ) -> N.Problem:
         nz, ny, nx = self.grid.shape
         p = N.Problem()
@@ -126,6 +127,7 @@ class RayPlan:
         p.field_dtype = field_dtype
         p.image_dtype = image_dtype
         p.layout = layout
+        p.block_cols = block_cols
         for k in range(9):
             p.object_to_grid[k] = self.object_to_grid[k]
         for k in range(3):

@@ -57,7 +57,9 @@ class ProjectionSpec:
     BF16 storage.  ``precision`` is the image / cotangent dtype.
     ``widen_views`` is how many views accumulate in FP32 before the volume
     gradient is widened into its FP64 total (the reference uses 8 for FP32 and 2
-    for FP64 sampling).
+    for FP64 sampling).  ``layout`` selects the corner-replicated field copy or
+    direct gathers; ``block_cols`` the detector tile of one 256-ray block (8, 16,
+    32 or 64 columns; 0 = 16), a launch-shape choice that does not change results.
     """
 
     samples_per_ray: int
@@ -68,6 +70,7 @@ class ProjectionSpec:
     storage_precision: StoragePrecision = "float32"
     widen_views: int | None = None
     layout: Literal["replicated", "direct"] = "replicated"
+    block_cols: int = 0
 
     def __post_init__(self) -> None:
         integer(self.samples_per_ray, "samples_per_ray", minimum=1)
@@ -87,6 +90,8 @@ class ProjectionSpec:
             raise ContractError("layout must be replicated or direct")
         if self.layout == "direct" and self.storage_precision != "float32":
             raise ContractError("the direct layout reads FP32 storage only")
+        if self.block_cols not in (0, 8, 16, 32, 64):
+            raise ContractError("block_cols must be 0 (default), 8, 16, 32 or 64")
 
     @property
     def arith(self) -> int:
@@ -143,6 +148,7 @@ class ProjectionWorkspace:
             field_dtype=spec.field_code,
             image_dtype=spec.image_code,
             layout=N.LAYOUT_DIRECT if spec.layout == "direct" else N.LAYOUT_REPLICATED,
+            block_cols=spec.block_cols,
         )
         with torch.cuda.device(device):
             self.view_table = (

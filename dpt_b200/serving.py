@@ -1,0 +1,519 @@
+"""Device-resident projection serving with continuous batching.
+
+The reference has no serving layer; this module is the request loop the B200 build
+adds on top of the projector:
+
+* volumes are registered once and stay resident (with their corner-replicated copy);
+* requests (forward, forward + volume VJP, forward + pose VJP) of any grid, view count,
+  detector and sample count arrive on a queue;
+* an admission loop starts a request as soon as a stream slot is free and its device
+  memory fits the budget (first fit over a bounded look-ahead, so a large request
+  waiting for memory does not block small ones behind it);
+* every admitted request runs on its own CUDA stream, so requests that arrive while
+  others are on the GPU overlap on the device;
+* repeated request shapes replay a captured CUDA graph of their launch sequence;
+* the detector tile of each request class comes from a small autotuner that times the
+  candidate tiles once per class and keeps the fastest.
+
+Results are exactly those of the same request run alone: the kernels are the same and
+requests share no scratch (each slot owns its workspaces).
+"""
+
+from __future__ import annotations
+
+import itertools
+import queue
+import threading
+import time
+from collections import OrderedDict, deque
+from collections.abc import Callable
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Any, Literal
+
+from .contracts import ContractError, integer
+
+RequestKind = Literal["forward", "volume", "pose"]
+
+
+@dataclass(frozen=True)
+class ProjectionRequest:
+    """One projection job against a registered volume.
+
+    ``kind``: ``"forward"`` returns the image; ``"volume"`` also returns the gradient of
+    ``0.5 * |image - target|^2`` with respect to the volume; ``"pose"`` the gradient with
+    respect to the per-view pose tangent.  ``target`` (host or device, image shape)
+    defaults to zeros.  ``tangent`` is an optional ``(views, 6)`` pose increment.
+    """
+
+    volume: str
+    geometry: Any
+    samples_per_ray: int
+    kind: RequestKind = "forward"
+    target: Any = None
+    tangent: Any = None
+    precision: Literal["fp32", "fp64"] = "fp32"
+
+    def __post_init__(self) -> None:
+        integer(self.samples_per_ray, "samples_per_ray", minimum=1)
+        if self.kind not in ("forward", "volume", "pose"):
+            raise ContractError("request kind must be forward, volume or pose")
+        if self.precision not in ("fp32", "fp64"):
+            raise ContractError("precision must be fp32 or fp64")
+
+
+@dataclass
+class ProjectionResult:
+    image: Any
+    loss: float | None = None
+    volume_gradient: Any = None
+    pose_gradient: Any = None
+    submitted: float = 0.0
+    started: float = 0.0
+    finished: float = 0.0
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.submitted
+
+
+class Admission:
+    """Memory-budget admission with a bounded first-fit look-ahead (no GPU needed).
+
+    ``offer(item, bytes)`` queues a request; ``take(free_slots)`` returns the requests that
+    can start now in arrival order, skipping (up to ``lookahead`` entries) those that do
+    not fit the remaining budget; ``release(bytes)`` returns memory when one finishes.
+    A request larger than the whole budget is rejected at ``offer``.
+    """
+
+    def __init__(self, budget_bytes: int, lookahead: int = 16) -> None:
+        if budget_bytes <= 0:
+            raise ContractError("memory budget must be positive")
+        self.budget = int(budget_bytes)
+        self.lookahead = lookahead
+        self.in_use = 0
+        self.peak = 0
+        self.waiting: deque[tuple[Any, int]] = deque()
+
+    def offer(self, item: Any, nbytes: int) -> None:
+        if nbytes > self.budget:
+            raise ContractError(f"request needs {nbytes} bytes, more than the {self.budget}-byte budget")
+        self.waiting.append((item, int(nbytes)))
+
+    def take(self, free_slots: int) -> list[tuple[Any, int]]:
+        started: list[tuple[Any, int]] = []
+        index = 0
+        while free_slots > 0 and index < min(len(self.waiting), self.lookahead):
+            item, nbytes = self.waiting[index]
+            if self.in_use + nbytes <= self.budget:
+                del self.waiting[index]
+                self.in_use += nbytes
+                self.peak = max(self.peak, self.in_use)
+                started.append((item, nbytes))
+                free_slots -= 1
+            else:
+                index += 1
+        return started
+
+    def release(self, nbytes: int) -> None:
+        self.in_use -= int(nbytes)
+        if self.in_use < 0:
+            raise ContractError("released more memory than was admitted")
+
+
+class TileTuner:
+    """Chooses the detector block tile (8, 16, 32 or 64 columns) per request class.
+
+    ``choose(key, run)`` calls ``run(block_cols)`` -> seconds once per candidate the
+    first time a class is seen and keeps the fastest; later calls return it directly.
+    """
+
+    CANDIDATES = (16, 32, 8, 64)
+
+    def __init__(self) -> None:
+        self.choices: dict[Any, int] = {}
+        self.timings: dict[Any, dict[int, float]] = {}
+        self.lock = threading.Lock()
+
+    def choose(self, key: Any, run: Callable[[int], float]) -> int:
+        with self.lock:
+            if key in self.choices:
+                return self.choices[key]
+        timings = {cols: run(cols) for cols in self.CANDIDATES}
+        best = min(timings, key=timings.get)
+        with self.lock:
+            self.timings[key] = timings
+            self.choices[key] = best
+        return best
+
+
+def percentile(values: list[float], q: float) -> float:
+    """Nearest-rank percentile (q in [0, 100])."""
+    if not values:
+        raise ContractError("no values")
+    ordered = sorted(values)
+    rank = max(1, min(len(ordered), int(-(-q * len(ordered) // 100))))
+    return ordered[rank - 1]
+
+
+# ----------------------------------------------------------------- the server
+
+
+@dataclass
+class _Volume:
+    grid: Any
+    field: Any  # device tensor, contiguous, storage dtype
+
+
+@dataclass
+class _Job:
+    request: ProjectionRequest
+    future: Future
+    submitted: float
+    nbytes: int = 0
+    slot: Any = None
+    started: float = 0.0
+    event: Any = None
+    outputs: dict = field(default_factory=dict)
+    workspace: Any = None
+
+
+class _Slot:
+    """One CUDA stream with its own workspaces (scratch is never shared across slots)."""
+
+    def __init__(self, torch, device, index: int) -> None:
+        self.index = index
+        self.stream = torch.cuda.Stream(device=device)
+        self.workspaces: OrderedDict[Any, Any] = OrderedDict()
+        self.graphs: dict[Any, Any] = {}
+        self.busy = False
+
+
+class ProjectionServer:
+    """Continuous-batching request loop over resident volumes on one GPU.
+
+    ``submit`` returns a ``concurrent.futures.Future`` resolving to a
+    ``ProjectionResult`` whose tensors stay on the device.  ``slots`` requests run
+    concurrently, each on its own stream; admission also respects
+    ``memory_budget_bytes`` (120 GiB by default).  ``graphs=True`` captures the
+    launch sequence of each (slot, request class) after its first run and replays it;
+    ``autotune=True`` picks the detector tile per request class.
+    """
+
+    def __init__(self, device: str = "cuda:0", *, memory_budget_bytes: int = 120 << 30, slots: int = 4,
+                 graphs: bool = True, autotune: bool = True, workspaces_per_slot: int = 8) -> None:
+        import torch
+
+        self.torch = torch
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ContractError("the projection server runs on a CUDA device")
+        integer(slots, "slots", minimum=1, maximum=64)
+        self.slots = [_Slot(torch, self.device, k) for k in range(slots)]
+        self.admission = Admission(memory_budget_bytes)
+        self.tuner = TileTuner()
+        self.graphs = graphs
+        self.autotune = autotune
+        self.workspaces_per_slot = workspaces_per_slot
+        self.volumes: dict[str, _Volume] = {}
+        self.lock = threading.Condition()
+        self.inbox: queue.Queue = queue.Queue()
+        self.running: deque[_Job] = deque()
+        self.closed = False
+        self.errors: list[BaseException] = []
+        self._scheduler = threading.Thread(target=self._schedule, name="dpt-schedule", daemon=True)
+        self._completer = threading.Thread(target=self._complete, name="dpt-complete", daemon=True)
+        self._scheduler.start()
+        self._completer.start()
+
+    # ----------------------------------------------------------- volumes
+    def add_volume(self, name: str, grid, values, storage: str = "float32") -> None:
+        """Upload (or adopt) a volume; it stays resident until ``remove_volume``."""
+        torch = self.torch
+        dtype = {"float32": torch.float32, "float16": torch.float16, "bfloat16": torch.bfloat16}[storage]
+        tensor = values if isinstance(values, torch.Tensor) else torch.as_tensor(values)
+        tensor = tensor.to(device=self.device, dtype=dtype).contiguous()
+        if tuple(tensor.shape) != tuple(grid.shape):
+            raise ContractError("volume values must have grid shape (nz, ny, nx)")
+        with self.lock:
+            self.volumes[name] = _Volume(grid, tensor)
+
+    def remove_volume(self, name: str) -> None:
+        with self.lock:
+            self.volumes.pop(name)
+            for slot in self.slots:
+                for key in [k for k in slot.workspaces if k[0] == name]:
+                    del slot.workspaces[key]
+                for key in [k for k in slot.graphs if k[0] == name]:
+                    del slot.graphs[key]
+
+    # -------------------------------------------------------------- API
+    def submit(self, request: ProjectionRequest) -> Future:
+        if request.volume not in self.volumes:
+            raise ContractError(f"unknown volume {request.volume!r}")
+        future: Future = Future()
+        job = _Job(request, future, time.perf_counter())
+        job.nbytes = self.request_bytes(request)
+        with self.lock:
+            if self.closed:
+                raise ContractError("server is closed")
+            self.admission.offer(job, job.nbytes)
+            self.lock.notify_all()
+        return future
+
+    def run_alone(self, request: ProjectionRequest) -> ProjectionResult:
+        """Run one request synchronously on the caller's stream (the sequential baseline)."""
+        job = _Job(request, Future(), time.perf_counter())
+        slot = _Slot(self.torch, self.device, -1)
+        slot.stream = self.torch.cuda.current_stream(self.device)
+        job.slot = slot
+        job.started = time.perf_counter()
+        self._launch(job, use_graph=False)
+        self.torch.cuda.current_stream(self.device).synchronize()
+        return self._finish(job)
+
+    def close(self) -> None:
+        with self.lock:
+            self.closed = True
+            self.lock.notify_all()
+        self._scheduler.join()
+        self._completer.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    # ---------------------------------------------------------- sizing
+    def request_bytes(self, request: ProjectionRequest) -> int:
+        from .plan import batched
+
+        volume = self.volumes[request.volume]
+        geometry = batched(request.geometry)
+        rays = geometry.pixels
+        image = 8 if request.precision == "fp64" else 4
+        total = 3 * rays * image + 4096
+        voxels = volume.grid.voxels
+        total += voxels * 16  # replicated field copy of this slot's workspace
+        if request.kind == "volume":
+            total += voxels * (32 + 8 + 4)
+        if request.kind == "pose":
+            total += len(geometry.views) * ((rays // len(geometry.views)) // 256 + 1) * 96 + 96 * rays // 256
+        return total
+
+    # ------------------------------------------------------- scheduling
+    def _schedule(self) -> None:
+        while True:
+            with self.lock:
+                while not self.closed and not self._startable():
+                    self.lock.wait(0.05)
+                if self.closed and not self.admission.waiting:
+                    return
+                free = [slot for slot in self.slots if not slot.busy]
+                taken = self.admission.take(len(free))
+                for (job, _), slot in zip(taken, free, strict=False):
+                    slot.busy = True
+                    job.slot = slot
+            for job, _ in taken:
+                try:
+                    job.started = time.perf_counter()
+                    self._launch(job, use_graph=self.graphs)
+                except BaseException as error:  # surfaced through the future
+                    job.outputs["error"] = error
+                    job.event = None
+                with self.lock:
+                    self.running.append(job)
+                    self.lock.notify_all()
+
+    def _startable(self) -> bool:
+        if not self.admission.waiting:
+            return False
+        return any(not slot.busy for slot in self.slots)
+
+    def _complete(self) -> None:
+        while True:
+            with self.lock:
+                while not self.running and not (self.closed and not self.admission.waiting
+                                                and not any(s.busy for s in self.slots)):
+                    self.lock.wait(0.05)
+                if not self.running:
+                    return
+                job = self.running.popleft()
+            if job.event is not None:
+                job.event.synchronize()
+            try:
+                if "error" in job.outputs:
+                    raise job.outputs["error"]
+                result = self._finish(job)
+                job.future.set_result(result)
+            except BaseException as error:
+                job.future.set_exception(error)
+            with self.lock:
+                job.slot.busy = False
+                self.admission.release(job.nbytes)
+                self.lock.notify_all()
+
+    # -------------------------------------------------------- execution
+    def _workspace(self, slot: _Slot, request: ProjectionRequest, block_cols: int):
+        from .plan import batched, plan_rays
+        from .projection import ProjectionSpec, ProjectionWorkspace
+
+        volume = self.volumes[request.volume]
+        geometry = batched(request.geometry)
+        key = (request.volume, geometry, request.samples_per_ray, request.precision, request.kind,
+               volume.field.dtype, block_cols)
+        found = slot.workspaces.get(key)
+        if found is None:
+            half = volume.field.dtype != self.torch.float32
+            sampling = "compensated" if half else ("float64" if request.precision == "fp64" else "float32")
+            storage = {self.torch.float16: "float16", self.torch.bfloat16: "bfloat16"}.get(volume.field.dtype,
+                                                                                          "float32")
+            spec = ProjectionSpec(request.samples_per_ray, active_pose=request.kind == "pose",
+                                  active_volume=request.kind == "volume",
+                                  precision="float64" if request.precision == "fp64" else "float32",
+                                  sampling_precision=sampling, storage_precision=storage,
+                                  block_cols=block_cols)
+            found = ProjectionWorkspace(plan_rays(volume.grid, geometry), spec, self.device)
+            slot.workspaces[key] = found
+            while len(slot.workspaces) > self.workspaces_per_slot:
+                slot.workspaces.popitem(last=False)
+        else:
+            slot.workspaces.move_to_end(key)
+        return key, found
+
+    def _poses(self, request: ProjectionRequest, views: int):
+        import numpy as np
+
+        from .geometry import RigidTransform, compose_pose
+
+        if request.tangent is None:
+            packed = np.tile(np.asarray(RigidTransform().packed()), (views, 1))
+        else:
+            tangent = np.asarray(request.tangent, dtype=np.float64).reshape(-1, 6)
+            tangent = np.broadcast_to(tangent, (views, 6))
+            packed = np.asarray([compose_pose(RigidTransform(), tuple(map(float, t))).packed()
+                                 for t in tangent])
+        return self.torch.tensor(packed, dtype=self.torch.float64)
+
+    def _block_cols(self, request: ProjectionRequest, slot: _Slot) -> int:
+        from .plan import batched
+
+        if not self.autotune:
+            return 0
+        volume = self.volumes[request.volume]
+        geometry = batched(request.geometry)
+        key = (volume.grid.shape, geometry.shape, request.samples_per_ray, request.kind, request.precision,
+               str(volume.field.dtype))
+        torch = self.torch
+
+        def run(cols: int) -> float:
+            _, ws = self._workspace(slot, request, cols)
+            poses = self._poses(request, len(geometry.views)).to(self.device)
+            with torch.cuda.stream(slot.stream):
+                ws.forward(volume.field, poses, checked=False)  # warm
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(slot.stream)
+                ws.forward(volume.field, poses, checked=False)
+                end.record(slot.stream)
+            end.synchronize()
+            ws.status.zero_()
+            return start.elapsed_time(end)
+
+        return self.tuner.choose(key, run)
+
+    def _launch(self, job: _Job, use_graph: bool) -> None:
+        torch = self.torch
+        request, slot = job.request, job.slot
+        block_cols = self._block_cols(request, slot) if slot.index >= 0 else 0
+        key, ws = self._workspace(slot, request, block_cols)
+        volume = self.volumes[request.volume]
+        views = ws.plan.views
+        with torch.cuda.stream(slot.stream):
+            poses_host = self._poses(request, views).pin_memory()
+            target = request.target
+            state = slot.graphs.get(key) if use_graph else None
+            if state is None:
+                inputs = {"poses": poses_host.to(self.device, non_blocking=True),
+                          "target": self._target(request, ws)}
+                outputs = self._body(ws, volume.field, inputs, request)
+                if use_graph:
+                    self._capture(slot, key, ws, volume.field, request, inputs)
+            else:
+                graph, inputs, outputs = state
+                inputs["poses"].copy_(poses_host, non_blocking=True)
+                if target is not None:
+                    inputs["target"].copy_(self._as_device(target), non_blocking=True)
+                else:
+                    inputs["target"].zero_()
+                graph.replay()
+                outputs = {name: value.clone() for name, value in outputs.items()}
+            status_host = torch.empty(views, dtype=torch.int32, pin_memory=True)
+            status_host.copy_(ws.status, non_blocking=True)
+            ws.status.zero_()
+            job.outputs = dict(outputs, status=status_host)
+            job.workspace = ws
+            job.event = torch.cuda.Event()
+            job.event.record(slot.stream)
+
+    def _as_device(self, value):
+        torch = self.torch
+        tensor = value if isinstance(value, torch.Tensor) else torch.as_tensor(value)
+        return tensor.to(self.device, non_blocking=True)
+
+    def _target(self, request: ProjectionRequest, ws):
+        torch = self.torch
+        if request.target is None:
+            return torch.zeros(ws.plan.image_shape, dtype=ws.spec.image_dtype, device=self.device)
+        return self._as_device(request.target).to(ws.spec.image_dtype).reshape(ws.plan.image_shape).clone()
+
+    def _body(self, ws, field_tensor, inputs, request: ProjectionRequest) -> dict:
+        """Launch sequence of one request on the current stream (no host synchronisation)."""
+        image = ws.forward(field_tensor, inputs["poses"], checked=False)
+        out = {"image": image}
+        if request.kind != "forward":
+            residual = image - inputs["target"]
+            out["loss"] = 0.5 * (residual.double() * residual.double()).sum()
+            if request.kind == "volume":
+                out["volume_gradient"], _ = ws.vjp(field_tensor, inputs["poses"], residual, volume=True,
+                                                   pose=None, checked=False)
+            else:
+                _, out["pose_gradient"] = ws.vjp(field_tensor, inputs["poses"], residual, volume=False,
+                                                 pose="tangent", checked=False)
+        return out
+
+    def _capture(self, slot: _Slot, key, ws, field_tensor, request, inputs) -> None:
+        torch = self.torch
+        static = {"poses": inputs["poses"].clone(), "target": inputs["target"].clone()}
+        graph = torch.cuda.CUDAGraph()
+        slot.stream.synchronize()
+        with torch.cuda.graph(graph, stream=slot.stream):
+            outputs = self._body(ws, field_tensor, static, request)
+        ws.status.zero_()
+        slot.graphs[key] = (graph, static, outputs)
+
+    def _finish(self, job: _Job) -> ProjectionResult:
+        from .contracts import NumericalError, raise_device_status
+
+        outputs = job.outputs
+        codes = outputs["status"].tolist()
+        for view, code in enumerate(codes):
+            if code:
+                try:
+                    raise_device_status(code, "projection")
+                except (ContractError, NumericalError) as error:
+                    error.args = (f"projection view {view}: {error}", *error.args[1:])
+                    raise
+        loss = outputs.get("loss")
+        return ProjectionResult(
+            image=outputs["image"],
+            loss=None if loss is None else float(loss),
+            volume_gradient=outputs.get("volume_gradient"),
+            pose_gradient=outputs.get("pose_gradient"),
+            submitted=job.submitted,
+            started=job.started,
+            finished=time.perf_counter(),
+        )
+
+
+_ids = itertools.count()

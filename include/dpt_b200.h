@@ -127,6 +127,8 @@ typedef struct dpt_problem {
     int32_t field_dtype;    /* DPT_F32, DPT_F16 or DPT_BF16 */
     int32_t image_dtype;    /* DPT_F32 or DPT_F64: image and cotangent element type */
     int32_t layout;         /* DPT_LAYOUT_*: how the sampling kernels read the field */
+    int32_t block_cols;     /* panels: detector columns per 256-ray block tile: 8, 16, 32 or 64
+                               (the tile is then 32, 16, 8 or 4 rows high); 0 selects 16 */
     double object_to_grid[9]; /* diag(1/h) G^T, row-major: grid index = M (x_object - origin) */
     double grid_origin[3];    /* object mm of sample (0,0,0) */
 } dpt_problem;

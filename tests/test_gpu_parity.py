@@ -162,3 +162,19 @@ def test_identity_pose_bundle_single_voxel_known_answer():
     volume, tangent = ws.vjp(field, pose, cot, volume=True, pose="tangent")
     np.testing.assert_allclose(volume.cpu().numpy().reshape(-1), [0.7], rtol=2e-5)
     np.testing.assert_allclose(tangent.cpu().numpy().reshape(-1), [-0.025, 0, 0, 0, 0, 0], rtol=2e-5, atol=1e-8)
+
+
+@pytest.mark.parametrize("block_cols", [8, 32, 64])
+def test_block_tile_shape_changes_no_result(block_cols):
+    grid, geometry, values = cone_scene(detector=(37, 45))
+    poses = poses_for(len(geometry.views), seed=11)
+    field, pose = device_inputs(values, poses)
+    base = workspace(grid, geometry, 29)
+    spec = ProjectionSpec(29, sampling_precision="float32", block_cols=block_cols)
+    tuned = ProjectionWorkspace(plan_rays(grid, geometry), spec, "cuda:0")
+    torch.testing.assert_close(tuned.forward(field, pose), base.forward(field, pose), rtol=0, atol=0)
+    cot = torch.rand(base.plan.image_shape, device="cuda:0")
+    v0, p0 = base.vjp(field, pose, cot, volume=True, pose="matrix")
+    v1, p1 = tuned.vjp(field, pose, cot, volume=True, pose="matrix")
+    assert rel_l2(v1.cpu().numpy(), v0.cpu().numpy()) < 1e-6
+    torch.testing.assert_close(p1, p0, rtol=1e-10, atol=1e-13)

@@ -1,0 +1,137 @@
+"""Serving: admission and tuning logic on the CPU; on the GPU, every request's result is
+the same alone and inside a concurrent mix (forward images bit-exact, gradients within
+the atomic-order tolerance), graph replays match first runs, and the budget holds."""
+
+from __future__ import annotations
+
+import math
+import random
+
+import numpy as np
+import pytest
+
+from dpt_b200.contracts import ContractError
+from dpt_b200.serving import Admission, ProjectionRequest, TileTuner, percentile
+
+
+def test_admission_first_fit_and_budget():
+    admission = Admission(100, lookahead=4)
+    for name, size in (("a", 60), ("b", 50), ("c", 30), ("d", 20)):
+        admission.offer(name, size)
+    started = admission.take(4)
+    assert [name for name, _ in started] == ["a", "c"]  # b waits for memory, c backfills
+    assert admission.in_use == 90
+    admission.release(60)
+    assert [name for name, _ in admission.take(4)] == ["b", "d"]  # 30 + 50 + 20 = 100 fits exactly
+    assert admission.in_use == 100 and not admission.waiting
+    with pytest.raises(ContractError):
+        admission.offer("huge", 101)
+    with pytest.raises(ContractError):
+        Admission(0)
+
+
+def test_admission_respects_slot_count_and_order():
+    admission = Admission(1000)
+    for k in range(10):
+        admission.offer(k, 10)
+    assert [k for k, _ in admission.take(3)] == [0, 1, 2]
+    assert [k for k, _ in admission.take(2)] == [3, 4]
+    assert admission.in_use == 50
+
+
+def test_tuner_times_each_candidate_once_and_keeps_the_fastest():
+    calls = []
+
+    def run(cols):
+        calls.append(cols)
+        return {8: 3.0, 16: 2.0, 32: 1.0, 64: 4.0}[cols]
+
+    tuner = TileTuner()
+    assert tuner.choose("k", run) == 32
+    assert tuner.choose("k", run) == 32
+    assert sorted(calls) == [8, 16, 32, 64]
+
+
+def test_percentiles_and_request_contracts():
+    values = list(range(1, 101))
+    assert percentile(values, 50) == 50 and percentile(values, 99) == 99 and percentile(values, 100) == 100
+    with pytest.raises(ContractError):
+        ProjectionRequest("v", None, 0)
+    with pytest.raises(ContractError):
+        ProjectionRequest("v", None, 8, kind="both")
+
+
+# ------------------------------------------------------------------- GPU
+
+
+def _scenes():
+    from dpt_b200.geometry import ConeBeamIntrinsics
+    from dpt_b200.phantoms import centred_grid, ellipsoid_phantom
+
+    out = {}
+    for name, shape, spacing in (("small", (20, 24, 28), 1.0), ("mid", (40, 36, 32), 0.8)):
+        grid = centred_grid(shape, (spacing,) * 3)
+        values, _ = ellipsoid_phantom(grid, seed=len(name), count=3)
+        out[name] = (grid, values)
+    return out, ConeBeamIntrinsics
+
+
+def _requests(seed: int = 3, count: int = 14):
+    from dpt_b200.serving import ProjectionRequest
+
+    scenes, intrinsics_type = _scenes()
+    rng = random.Random(seed)
+    requests = []
+    for _ in range(count):
+        name = rng.choice(sorted(scenes))
+        views = rng.choice((1, 2, 5))
+        detector = rng.choice((16, 24, 40))
+        intrinsics = intrinsics_type(120.0, 200.0, (detector, detector), (1.6, 1.6))
+        geometry = intrinsics.batch(tuple(2 * math.pi * k / views + 0.3 for k in range(views)))
+        kind = rng.choice(("forward", "forward", "volume", "pose"))
+        target = np.full((views, detector, detector), 0.05, dtype=np.float32)
+        tangent = np.asarray([0.2, -0.1, 0.05, 0.01, 0.0, -0.02]) if kind == "pose" else None
+        requests.append(ProjectionRequest(name, geometry, rng.choice((32, 48)), kind, target, tangent))
+    return scenes, requests
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graphs", [False, True])
+def test_results_are_the_same_alone_and_in_the_mix(graphs):
+    from dpt_b200.serving import ProjectionServer
+
+    scenes, requests = _requests()
+    with ProjectionServer("cuda:0", slots=4, graphs=graphs, autotune=graphs) as server:
+        for name, (grid, values) in scenes.items():
+            server.add_volume(name, grid, values)
+        alone = [server.run_alone(request) for request in requests]
+        futures = [server.submit(request) for request in requests + requests]
+        mixed = [future.result(timeout=300) for future in futures]
+    for k, request in enumerate(requests + requests):
+        a, m = alone[k % len(requests)], mixed[k]
+        np.testing.assert_array_equal(m.image.cpu().numpy(), a.image.cpu().numpy())
+        if request.kind == "volume":
+            va, vm = a.volume_gradient.cpu().numpy(), m.volume_gradient.cpu().numpy()
+            assert np.linalg.norm(va - vm) <= 1e-6 * np.linalg.norm(va)
+        if request.kind == "pose":
+            np.testing.assert_allclose(m.pose_gradient.cpu().numpy(), a.pose_gradient.cpu().numpy(),
+                                       rtol=1e-10, atol=1e-13)
+        if request.kind != "forward":
+            assert m.loss == pytest.approx(a.loss, rel=1e-12)
+        assert m.latency > 0
+
+
+@pytest.mark.gpu
+def test_budget_limits_concurrency():
+    from dpt_b200.serving import ProjectionServer
+
+    scenes, requests = _requests(seed=5, count=6)
+    with ProjectionServer("cuda:0", slots=4, graphs=False, autotune=False) as server:
+        for name, (grid, values) in scenes.items():
+            server.add_volume(name, grid, values)
+        largest = max(server.request_bytes(r) for r in requests)
+        server.admission.budget = largest  # one request at a time fits
+        results = [f.result(timeout=300) for f in [server.submit(r) for r in requests]]
+    assert len(results) == len(requests)
+    assert server.admission.peak <= largest
+    assert server.admission.in_use == 0
