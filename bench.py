@@ -58,6 +58,9 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--storage", choices=("float32", "bfloat16", "float16"), default="float32")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--seed", type=int, default=20261203)
+    parser.add_argument("--mode", choices=("iteration", "serving"), default="iteration",
+                        help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
+    parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
     return parser.parse_args()
 
 
@@ -435,10 +438,103 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def serving_requests(args, device):
+    """Seeded mixed request stream: resident volumes of 64^3, 128^3, 256^3 and 512x512x128 in
+    FP32 or BF16, 1-64 views (log-uniform), square detectors 128^2-1024^2, 128-1024 samples;
+    60% forward, 30% forward + volume VJP, 10% forward + pose VJP; Poisson arrivals."""
+    import numpy as np
+
+    from dpt_b200.geometry import ConeBeamIntrinsics
+    from dpt_b200.phantoms import centred_grid, chest_phantom
+    from dpt_b200.serving import ProjectionRequest
+
+    rng = np.random.default_rng(args.seed)
+    volumes = {}
+    for name, shape, spacing in (("v64", (64, 64, 64), 3.2), ("v128", (128, 128, 128), 1.6),
+                                 ("v256", (256, 256, 256), 0.8), ("v512", (128, 512, 512), 0.4)):
+        grid = centred_grid(shape, (spacing, spacing, spacing * (4.0 if name == "v512" else 1.0)))
+        volumes[name] = (grid, chest_phantom(grid, seed=args.seed))
+    requests = []
+    for _ in range(args.requests):
+        name = ("v64", "v128", "v256", "v512")[int(rng.integers(4))]
+        storage = "bfloat16" if rng.random() < 0.5 else "float32"
+        views = int(round(math.exp(rng.uniform(0.0, math.log(64.0)))))
+        detector = int(rng.choice((128, 256, 512, 1024)))
+        samples = int(rng.choice((128, 256, 512, 1024)))
+        kind = ("forward", "volume", "pose")[int(rng.choice(3, p=(0.6, 0.3, 0.1)))]
+        pitch = 409.6 / detector
+        geometry = ConeBeamIntrinsics(1000.0, 1500.0, (detector, detector), (pitch, pitch)).batch(
+            tuple(2.0 * math.pi * k / views + float(rng.uniform(0, 0.1)) for k in range(views)))
+        requests.append((ProjectionRequest(f"{name}:{storage}", geometry, samples, kind), storage, name))
+    return volumes, requests
+
+
+def run_serving(args) -> None:
+    """Served mixed stream vs the same requests run one after another."""
+    import numpy as np
+    import torch
+
+    from dpt_b200.serving import ProjectionServer, percentile
+
+    device = torch.device("cuda:0")
+    volumes, stream = serving_requests(args, device)
+    with ProjectionServer(str(device), slots=4) as server:
+        for name, (grid, values) in volumes.items():
+            for storage in ("float32", "bfloat16"):
+                server.add_volume(f"{name}:{storage}", grid, values, storage=storage)
+        requests = [request for request, _, _ in stream]
+        samples_total = 0
+        for request in requests:
+            server.run_alone(request)  # warm-up: workspaces, packed copies
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        for request in requests:
+            server.run_alone(request)
+        torch.cuda.synchronize()
+        sequential_s = time.perf_counter() - start
+        for request in requests:  # warm the served path too (graphs, tiles)
+            server.submit(request).result()
+        rng = np.random.default_rng(args.seed + 7)
+        rate = 1.5 * len(requests) / sequential_s
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(requests)))
+        start = time.perf_counter()
+        futures = []
+        for request, arrival in zip(requests, arrivals, strict=True):
+            delay = start + arrival - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futures.append(server.submit(request))
+        results = [future.result() for future in futures]
+        served_s = max(r.finished for r in results) - start
+    latencies = [r.latency * 1e3 for r in results]
+    for request in requests:
+        rays = sum(v.pixels for v in request.geometry.views)
+        samples_total += rays * request.samples_per_ray
+    line = {
+        "metric": "served mixed projection stream",
+        "value": len(requests) / served_s,
+        "unit": "requests/s",
+        "sequential_requests_per_s": len(requests) / sequential_s,
+        "speedup_vs_sequential": sequential_s / served_s,
+        "p50_ms": percentile(latencies, 50),
+        "p99_ms": percentile(latencies, 99),
+        "requests": len(requests),
+        "nominal_ray_samples": samples_total,
+        "arrival_rate_per_s": rate,
+        "higher_is_better": True,
+        "config": {"workload": "Poisson mix: 64^3/128^3/256^3/512x512x128 volumes FP32|BF16, 1-64 views, "
+                               "128^2-1024^2 detectors, S 128-1024, 60/30/10 forward/volume/pose",
+                   "slots": 4, "memory_budget_gib": 120},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "serving":
+        run_serving(args)
     else:
         run_gpu(args)
 

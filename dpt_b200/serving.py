@@ -377,7 +377,9 @@ class ProjectionServer:
             found = ProjectionWorkspace(plan_rays(volume.grid, geometry), spec, self.device)
             slot.workspaces[key] = found
             while len(slot.workspaces) > self.workspaces_per_slot:
-                slot.workspaces.popitem(last=False)
+                evicted, _ = slot.workspaces.popitem(last=False)
+                # a captured graph points into its workspace's scratch: drop them together
+                slot.graphs.pop(evicted, None)
         else:
             slot.workspaces.move_to_end(key)
         return key, found

@@ -143,7 +143,7 @@ def test_per_ray_pose_rows_sum_to_view_gradient():
     _, tangent = ws.vjp(field, pose, cot, volume=False, pose="tangent")
     per_view = rows.reshape(2, -1, 6).sum(axis=1)
     np.testing.assert_allclose(per_view, tangent.cpu().numpy(), rtol=1e-10, atol=1e-13)
-    e_rows, _, _ = O.vjp(ws.plan, values, poses, seed, samples=40, flags=O.VJP_PER_RAY6)
+    _, e_rows, _ = O.vjp(ws.plan, values, poses, seed, samples=40, flags=O.VJP_PER_RAY6)
     np.testing.assert_array_equal(rows, e_rows)
 
 

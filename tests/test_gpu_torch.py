@@ -165,15 +165,27 @@ def test_invalid_inputs_raise_typed_errors_and_the_next_call_recovers():
 
 
 def test_half_storage_fields_through_the_projector():
+    """FP16/BF16 fields run the compensated arithmetic on their decoded values: bit-identical
+    to the compensated form on the decoded FP32 field, and within 1e-5 relative L2 of the
+    FP32 reference-arithmetic projector."""
+    from dpt_b200.plan import plan_rays
+    from dpt_b200.projection import ProjectionSpec, ProjectionWorkspace
+
     grid, geometry, values = cone_scene()
     module = Projector(grid=grid, geometry=geometry, precision="fp32", samples_per_ray=64)
+    compensated = ProjectionWorkspace(plan_rays(grid, geometry),
+                                      ProjectionSpec(64, sampling_precision="compensated"), DEVICE)
+    identity = torch.tensor(RigidTransform().packed(), dtype=torch.float64, device=DEVICE)
+    poses = identity.expand(len(geometry.views), 12).contiguous()
     reference_field = torch.tensor(values, device=DEVICE)
     for dtype in (torch.bfloat16, torch.float16):
         half = reference_field.to(dtype).requires_grad_()
         decoded = half.detach().float().requires_grad_()
         image = module(half)
+        torch.testing.assert_close(image, compensated.forward(decoded.detach(), poses), rtol=0, atol=0)
         baseline = module(decoded)
-        torch.testing.assert_close(image, baseline, rtol=2e-6, atol=2e-7)
+        error = (image - baseline).norm() / baseline.norm()
+        assert error < 1e-5, float(error)
         image.sum().backward()
         baseline.sum().backward()
         assert half.grad.dtype == dtype
