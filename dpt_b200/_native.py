@@ -38,6 +38,7 @@ EXPORTS = (
     "dpt_b200_finish_pose",
     "dpt_b200_fold_volume",
     "dpt_b200_counts",
+    "dpt_b200_pose_vjp_fixed",
 )
 
 
@@ -93,6 +94,7 @@ _SIGNATURES = {
     "dpt_b200_finish_pose": ([_P, _I, _I, _I, _V, _V, _I, _V, _V], ctypes.c_int),
     "dpt_b200_fold_volume": ([_P, _V, _V, _I, _V, _I, _I, _V, _V], ctypes.c_int),
     "dpt_b200_counts": ([_P, _R, _V, _V, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_pose_vjp_fixed": ([_P, _R, _V, _V, _I, _V, _V, _V], ctypes.c_int),
 }
 
 _lock = threading.Lock()

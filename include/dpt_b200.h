@@ -196,6 +196,19 @@ int dpt_b200_fold_volume(const dpt_problem* problem, float* accumulator, double*
 int dpt_b200_counts(const dpt_problem* problem, const dpt_rays* rays, double* lower,
                     double* upper, int32_t* realised, int32_t* status, void* stream);
 
+/* Pose cotangent of views [view_begin, view_begin+view_count) without any caller scratch
+ * and without allocating: for callers that cannot call cudaMalloc while they run (a
+ * guidance or tracking loop that reserves its device memory up front, or a plugin whose
+ * host application owns the GPU memory).  No counterpart in the reference.  The per-block
+ * partials live in a fixed 1 MiB device array inside the library (view_count x blocks per
+ * view x components <= 131072, else DPT_E_CAPACITY); the FP32 field is read directly.
+ * The first call on a device looks up that array's address (call it once before any stream
+ * capture); calls that overlap on the GPU share the array and race.  `pose_gradient` is
+ * view_count x components (12 packed or 6 local-right); status as dpt_b200_vjp. */
+int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_rays* rays, const float* field,
+                            const void* cotangent, int32_t components, double* pose_gradient,
+                            int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
