@@ -422,6 +422,74 @@ __device__ __forceinline__ void slope64(double fx, double fy, double fz, const d
     g[2] = sz * fma(fy, dz1, ay * dz0);
 }
 
+// Grid bounds used by every sample (computed once per thread).
+struct FieldDims {
+    int nx, ny, nz;
+    float hx, hy, hz;   // n - 0.5: upper end of the half-cell support
+    float mx, my, mz;   // n - 1: clamp bound
+    int cx, cy, cz;     // max(n - 2, 0): largest lower cell index
+    __device__ __forceinline__ void init(const Grid& g)
+    {
+        nx = g.nx; ny = g.ny; nz = g.nz;
+        hx = (float)nx - 0.5f; hy = (float)ny - 0.5f; hz = (float)nz - 0.5f;
+        mx = (float)(nx - 1); my = (float)(ny - 1); mz = (float)(nz - 1);
+        cx = max(nx - 2, 0); cy = max(ny - 2, 0); cz = max(nz - 2, 0);
+    }
+};
+
+// A ray whose grid-space origin and direction are below 1e30 in magnitude has only finite
+// sample points (each point is o + t d with t in [0, 1]), so its samples need no finiteness
+// test; other rays take the general path.
+__device__ __forceinline__ bool moderate(const float* o, const float* d)
+{
+    const float m = fmaxf(fmaxf(fmaxf(fabsf(o[0]), fabsf(o[1])), fmaxf(fabsf(o[2]), fabsf(d[0]))),
+                          fmaxf(fabsf(d[1]), fabsf(d[2])));
+    return m < 1e30f;
+}
+__device__ __forceinline__ bool moderate(const double* o, const double* d)
+{
+    const double m = fmax(fmax(fmax(fabs(o[0]), fabs(o[1])), fmax(fabs(o[2]), fabs(d[0]))),
+                          fmax(fabs(d[1]), fabs(d[2])));
+    return m < 1e300;
+}
+
+// The midpoints of one ray are monotone in the sample index along every axis (each point
+// is an fma that is monotone in its sample parameter), so the samples inside the half-cell
+// support form one contiguous run.  Find its ends [first, last] (first > last when empty);
+// samples outside the run contribute exactly zero and need not be visited.
+template <typename Inside>
+__device__ __forceinline__ void inside_run(int samples, Inside inside_at, int& first, int& last)
+{
+    first = 0;
+    last = samples - 1;
+    while (first <= last && !inside_at(first)) ++first;
+    while (last > first && !inside_at(last)) --last;
+}
+
+// Last cell's eight corner values, reloaded only when the sample enters another cell.
+template <class Field>
+struct CellCache {
+    float v[8];
+    int cell = -1;
+    __device__ __forceinline__ void fetch(const Field& f, int lx, int ly, int lz, int index)
+    {
+        if (index != cell) {
+            f.load(lx, ly, lz, v);
+            cell = index;
+        }
+    }
+};
+
+// FP32 product with results below the normal range flushed to signed zero: the scatter
+// increment of the reference (a rounded product, then |x| < 2^-126 -> 0, as CUDA's global
+// FP32 atomics treat subnormal operands), in one instruction.
+__device__ __forceinline__ float mul_ftz(float a, float b)
+{
+    float r;
+    asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
 // Per-block staging of the view's pose (12 doubles) and panel record.
 struct ViewShared {
     double pose[12];

@@ -17,20 +17,6 @@
 namespace dpt {
 namespace {
 
-struct FieldDims {
-    int nx, ny, nz;
-    float hx, hy, hz;   // n - 0.5 (support upper bound)
-    float mx, my, mz;   // n - 1 (clamp bound)
-    int cx, cy, cz;     // max(n - 2, 0) (lower-cell cap)
-    __device__ __forceinline__ void init(const Grid& g)
-    {
-        nx = g.nx; ny = g.ny; nz = g.nz;
-        hx = (float)nx - 0.5f; hy = (float)ny - 0.5f; hz = (float)nz - 0.5f;
-        mx = (float)(nx - 1); my = (float)(ny - 1); mz = (float)(nz - 1);
-        cx = max(nx - 2, 0); cy = max(ny - 2, 0); cz = max(nz - 2, 0);
-    }
-};
-
 // FP32 sample of the field at grid point (x, y, z): zero outside the half-cell support.
 template <class Field>
 __device__ __forceinline__ float sample32(const Field& f, const FieldDims& d, float x, float y,
@@ -98,17 +84,43 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                 FieldDims dims;
                 dims.init(a.grid);
                 const float step = (iv.upper - iv.lower) / (float)S;
-                bool finite = true;
-#pragma unroll 4
-                for (int i = 0; i < S; ++i) {
+                auto at = [&](int i, float& x, float& y, float& z) {
                     const float position = fmaf((float)i + 0.5f, step, iv.lower);
-                    const float x = fmaf(position, d[0], o[0]);
-                    const float y = fmaf(position, d[1], o[1]);
-                    const float z = fmaf(position, d[2], o[2]);
-                    finite = finite && finite3f(x, y, z);
-                    total = total + sample32(f, dims, x, y, z);
+                    x = fmaf(position, d[0], o[0]);
+                    y = fmaf(position, d[1], o[1]);
+                    z = fmaf(position, d[2], o[2]);
+                };
+                if (!moderate(o, d)) {
+                    bool finite = true;
+                    for (int i = 0; i < S; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        finite = finite && finite3f(x, y, z);
+                        total = total + sample32(f, dims, x, y, z);
+                    }
+                    if (!finite) bits |= 2;
+                } else {
+                    int first, last;
+                    inside_run(S, [&](int i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        return inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                    }, first, last);
+                    CellCache<Field> cache;
+#pragma unroll 4
+                    for (int i = first; i <= last; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        const Axis32 X = axis32(x, dims.mx, dims.cx), Y = axis32(y, dims.my, dims.cy),
+                                     Z = axis32(z, dims.mz, dims.cz);
+                        cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
+                        float w[8];
+                        corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+                        total = total + interpolate(w, cache.v);
+                    }
+                    // the zero samples after the run: adding +0 only turns -0 into +0
+                    if (last < S - 1) total = total + 0.0f;
                 }
-                if (!finite) bits |= 2;
                 total = total * (length * step);
             }
             if (!isfinite(total)) bits |= 2;
@@ -123,17 +135,43 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
             double integral = 0.0;
             if (iv.upper > iv.lower) {
                 const double step = (iv.upper - iv.lower) / (double)S;
-                bool finite = true;
-#pragma unroll 2
-                for (int i = 0; i < S; ++i) {
+                auto at = [&](int i, double* p) {
                     const double position = fma((double)i + 0.5, step, iv.lower);
-                    double p[3];
 #pragma unroll
                     for (int k = 0; k < 3; ++k) p[k] = fma(position, r.direction[k], r.origin[k]);
-                    finite = finite && finite3(p[0], p[1], p[2]);
-                    integral = integral + sample64(f, a.grid, p);
+                };
+                if (!moderate(r.origin, r.direction)) {
+                    bool finite = true;
+                    for (int i = 0; i < S; ++i) {
+                        double p[3];
+                        at(i, p);
+                        finite = finite && finite3(p[0], p[1], p[2]);
+                        integral = integral + sample64(f, a.grid, p);
+                    }
+                    if (!finite) bits |= 2;
+                } else {
+                    int first, last;
+                    inside_run(S, [&](int i) {
+                        double p[3];
+                        at(i, p);
+                        return inside(p[0], p[1], p[2], a.grid.nx, a.grid.ny, a.grid.nz);
+                    }, first, last);
+                    const double mx = (double)(a.grid.nx - 1), my = (double)(a.grid.ny - 1), mz = (double)(a.grid.nz - 1);
+                    const int cx = max(a.grid.nx - 2, 0), cy = max(a.grid.ny - 2, 0), cz = max(a.grid.nz - 2, 0);
+                    CellCache<Field> cache;
+#pragma unroll 2
+                    for (int i = first; i <= last; ++i) {
+                        double p[3];
+                        at(i, p);
+                        const Axis64 X = axis64(p[0], mx, cx), Y = axis64(p[1], my, cy), Z = axis64(p[2], mz, cz);
+                        cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * a.grid.ny + Y.lower) * a.grid.nx + X.lower);
+                        double v[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) v[c] = (double)cache.v[c];
+                        integral = integral + interpolate64(X.fraction, Y.fraction, Z.fraction, v);
+                    }
+                    if (last < S - 1) integral = integral + 0.0;
                 }
-                if (!finite) bits |= 2;
                 integral = integral * (r.length * step);
             }
             result = integral;
@@ -156,21 +194,49 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                     sv[k] = (float)(step * r.direction[k]);
                 }
                 float sum = 0.0f, carry = 0.0f;
-                bool finite = true;
-#pragma unroll 4
-                for (int i = 0; i < S; ++i) {
+                auto at = [&](int i, float& x, float& y, float& z) {
                     const float offset = (float)i + 0.5f;
-                    const float x = fmaf(offset, sv[0], entry[0]);
-                    const float y = fmaf(offset, sv[1], entry[1]);
-                    const float z = fmaf(offset, sv[2], entry[2]);
-                    finite = finite && finite3f(x, y, z);
-                    const float value = sample32(f, dims, x, y, z);
+                    x = fmaf(offset, sv[0], entry[0]);
+                    y = fmaf(offset, sv[1], entry[1]);
+                    z = fmaf(offset, sv[2], entry[2]);
+                };
+                auto add = [&](float value) {
                     const float yk = value - carry;
                     const float t = sum + yk;
                     carry = (t - sum) - yk;
                     sum = t;
+                };
+                if (!moderate(entry, sv)) {
+                    bool finite = true;
+                    for (int i = 0; i < S; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        finite = finite && finite3f(x, y, z);
+                        add(sample32(f, dims, x, y, z));
+                    }
+                    if (!finite) bits |= 2;
+                } else {
+                    int first, last;
+                    inside_run(S, [&](int i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        return inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                    }, first, last);
+                    CellCache<Field> cache;
+#pragma unroll 4
+                    for (int i = first; i <= last; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        const Axis32 X = axis32(x, dims.mx, dims.cx), Y = axis32(y, dims.my, dims.cy),
+                                     Z = axis32(z, dims.mz, dims.cz);
+                        cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
+                        float w[8];
+                        corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+                        add(interpolate(w, cache.v));
+                    }
+                    // zero samples after the run still move the compensation into the sum
+                    for (int i = max(last + 1, first); i < S; ++i) add(0.0f);
                 }
-                if (!finite) bits |= 2;
                 result = ((double)sum - (double)carry) * (r.length * step);
             }
             if (!finite_out<Out>(result)) bits |= 2;

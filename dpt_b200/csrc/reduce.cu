@@ -9,8 +9,8 @@
 // total.  This is where the FP32 per-batch sums are widened to FP64, as the reference
 // does every 8 views (python/dpt/torch/_projection_ops.py:304-352).  The final pass also
 // scans the gradient for non-finite values (reference python/dpt/projection.py:470-499).
-// Every accumulator slot is read by exactly one voxel thread, so the same thread clears
-// it for the next batch.
+// The cell records of a 16x4x4 voxel tile are staged through shared memory with coalesced
+// loads; the accumulator is then cleared for the next batch with one memset.
 #include "launch.h"
 
 namespace dpt {
@@ -59,31 +59,55 @@ __device__ __forceinline__ int axis_sources(int x, int n, int* cells, int* bits)
     return count;
 }
 
+// Fold tile: 16 x 4 x 4 voxels per 256-thread block.  The cells that touch those voxels are
+// [x0-1, x0+16) x [y0-1, y0+4) x [z0-1, z0+4): 17 x 5 x 5 records of 32 bytes, loaded into
+// shared memory with coalesced 16-byte loads (about 1.7 record reads per voxel).
+constexpr int kFoldX = 16, kFoldY = 4, kFoldZ = 4;
+constexpr int kHaloX = kFoldX + 1, kHaloY = kFoldY + 1, kHaloZ = kFoldZ + 1;
+constexpr int kHaloCells = kHaloX * kHaloY * kHaloZ;
+
 template <typename G>
-__global__ void __launch_bounds__(256) k_fold(int nx, int ny, int nz, float* __restrict__ acc,
+__global__ void __launch_bounds__(256) k_fold(int nx, int ny, int nz, const float* __restrict__ acc,
                                               double* __restrict__ total, int accumulate_total,
-                                              G* __restrict__ gradient, int clear, int32_t* status)
+                                              G* __restrict__ gradient, int32_t* status)
 {
-    const int64_t voxels = (int64_t)nx * ny * nz;
-    const int64_t index = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float4 cells[kHaloCells][2];
+    const int tiles_x = (nx + kFoldX - 1) / kFoldX, tiles_y = (ny + kFoldY - 1) / kFoldY;
+    const int tile = blockIdx.x;
+    const int tz = tile / (tiles_x * tiles_y), rest = tile - tz * tiles_x * tiles_y;
+    const int ty = rest / tiles_x, tx = rest - ty * tiles_x;
+    const int x0 = tx * kFoldX, y0 = ty * kFoldY, z0 = tz * kFoldZ;
+    const float4* records = reinterpret_cast<const float4*>(acc);
+    for (int i = threadIdx.x; i < 2 * kHaloCells; i += 256) {
+        const int half = i & 1, c = i >> 1;
+        const int cz = c / (kHaloX * kHaloY), cr = c - cz * kHaloX * kHaloY;
+        const int cy = cr / kHaloX, cx = cr - cy * kHaloX;
+        const int gx = x0 - 1 + cx, gy = y0 - 1 + cy, gz = z0 - 1 + cz;
+        float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (gx >= 0 && gy >= 0 && gz >= 0 && gx < nx && gy < ny && gz < nz)
+            value = __ldg(records + 2 * (((int64_t)gz * ny + gy) * nx + gx) + half);
+        cells[c][half] = value;
+    }
+    __syncthreads();
+    const int lx = threadIdx.x % kFoldX, ly = (threadIdx.x / kFoldX) % kFoldY, lz = threadIdx.x / (kFoldX * kFoldY);
+    const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
     bool bad = false;
-    if (index < voxels) {
-        const int x = (int)(index % nx);
-        const int64_t rest = index / nx;
-        const int y = (int)(rest % ny), z = (int)(rest / ny);
-        int cx[2], bx[2], cy[2], by[2], cz[2], bz[2];
-        const int kx = axis_sources(x, nx, cx, bx);
-        const int ky = axis_sources(y, ny, cy, by);
-        const int kz = axis_sources(z, nz, cz, bz);
+    if (x < nx && y < ny && z < nz) {
+        int cxs[2], bxs[2], cys[2], bys[2], czs[2], bzs[2];
+        const int kx = axis_sources(x, nx, cxs, bxs);
+        const int ky = axis_sources(y, ny, cys, bys);
+        const int kz = axis_sources(z, nz, czs, bzs);
         double sum = 0.0;
         for (int iz = 0; iz < kz; ++iz)
             for (int iy = 0; iy < ky; ++iy)
                 for (int ix = 0; ix < kx; ++ix) {
-                    const int64_t cell = ((int64_t)cz[iz] * ny + cy[iy]) * nx + cx[ix];
-                    float* slot = acc + 8 * cell + (bx[ix] | (by[iy] << 1) | (bz[iz] << 2));
-                    sum += (double)*slot;
-                    if (clear) *slot = 0.0f;
+                    const int c = ((czs[iz] - z0 + 1) * kHaloY + (cys[iy] - y0 + 1)) * kHaloX + (cxs[ix] - x0 + 1);
+                    const int corner = bxs[ix] | (bys[iy] << 1) | (bzs[iz] << 2);
+                    const float4 q = cells[c][corner >> 2];
+                    const int k = corner & 3;
+                    sum += (double)(k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w);
                 }
+        const int64_t index = ((int64_t)z * ny + y) * nx + x;
         double value = sum;
         if (total) {
             if (accumulate_total) value += total[index];
@@ -114,17 +138,18 @@ cudaError_t launch_fold(const dpt_problem& p, float* accumulator, double* total,
                         int accumulate_total, void* gradient, int gradient_dtype, int clear,
                         int32_t* status, cudaStream_t stream)
 {
-    const int64_t voxels = (int64_t)p.nx * p.ny * p.nz;
-    const unsigned blocks = (unsigned)((voxels + 255) / 256);
+    const unsigned blocks = (unsigned)(((p.nx + kFoldX - 1) / kFoldX) * ((p.ny + kFoldY - 1) / kFoldY) *
+                                       ((p.nz + kFoldZ - 1) / kFoldZ));
     if (gradient_dtype == DPT_F64)
         k_fold<double><<<blocks, 256, 0, stream>>>(p.nx, p.ny, p.nz, accumulator, total,
-                                                   accumulate_total, static_cast<double*>(gradient),
-                                                   clear, status);
+                                                   accumulate_total, static_cast<double*>(gradient), status);
     else
         k_fold<float><<<blocks, 256, 0, stream>>>(p.nx, p.ny, p.nz, accumulator, total,
-                                                  accumulate_total, static_cast<float*>(gradient),
-                                                  clear, status);
-    return cudaGetLastError();
+                                                  accumulate_total, static_cast<float*>(gradient), status);
+    cudaError_t error = cudaGetLastError();
+    if (error == cudaSuccess && clear)
+        error = cudaMemsetAsync(accumulator, 0, (size_t)p.nx * p.ny * p.nz * 32u, stream);
+    return error;
 }
 
 }  // namespace dpt

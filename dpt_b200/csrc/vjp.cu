@@ -20,18 +20,7 @@
 namespace dpt {
 namespace {
 
-struct Dims {
-    int nx, ny, nz;
-    float hx, hy, hz, mx, my, mz;
-    int cx, cy, cz;
-    __device__ __forceinline__ void init(const Grid& g)
-    {
-        nx = g.nx; ny = g.ny; nz = g.nz;
-        hx = (float)nx - 0.5f; hy = (float)ny - 0.5f; hz = (float)nz - 0.5f;
-        mx = (float)(nx - 1); my = (float)(ny - 1); mz = (float)(nz - 1);
-        cx = max(nx - 2, 0); cy = max(ny - 2, 0); cz = max(nz - 2, 0);
-    }
-};
+constexpr int kAlphaTable = 2048;
 
 __device__ __forceinline__ void flush_cell(float* acc, int cell, const float* cs)
 {
@@ -91,8 +80,15 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
 {
     __shared__ ViewShared vs;
     __shared__ double warp_sums[kBlock / 32][12];
+    // alpha_i = (i + 0.5) / S of the FP32 pose moments, each one IEEE division, tabulated
+    // once per block for the first kAlphaTable samples (later samples divide directly)
+    __shared__ float alpha_table[kArith == DPT_ARITH_F32 && kPose ? kAlphaTable : 1];
     const int view_local = blockIdx.y;
     const int view = a.view_begin + view_local;
+    if (kArith == DPT_ARITH_F32 && kPose) {
+        const int n = min(a.samples, kAlphaTable);
+        for (int k = threadIdx.x; k < n; k += kBlock) alpha_table[k] = ((float)k + 0.5f) / (float)a.samples;
+    }
     stage_view(a, view, vs);
     int pixel;
     const bool active = ray_of_thread(a, blockIdx.x, &pixel);
@@ -109,7 +105,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
         Ray64 r;
         ray_setup(a.grid, vs.pose, source, end, r);
         const double seed_in = (double)cot[view_local * rays_per_view + pixel];
-        Dims dims;
+        FieldDims dims;
         dims.init(a.grid);
 
         if (kArith == DPT_ARITH_F32) {
@@ -136,33 +132,39 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
 #pragma unroll
                     for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                     int pending = -1;
-                    bool finite = true;
-#pragma unroll 2
-                    for (int i = 0; i < S; ++i) {
-                        const float position = fmaf((float)i + 0.5f, step, iv.lower);
+                    CellCache<Field> cache;
+                    auto position_at = [&](int i) { return fmaf((float)i + 0.5f, step, iv.lower); };
+                    // One midpoint; `known_inside` is true on the inside run, where the support
+                    // and finiteness tests are known to pass.
+                    auto visit = [&](int i, bool known_inside) {
+                        const float position = position_at(i);
                         const float x = fmaf(position, d[0], o[0]);
                         const float y = fmaf(position, d[1], o[1]);
                         const float z = fmaf(position, d[2], o[2]);
-                        finite = finite && finite3f(x, y, z);
-                        const bool in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                        bool in = true;
+                        if (!known_inside) {
+                            if (!finite3f(x, y, z)) bits |= 2;
+                            in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                        }
                         Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
                         float w[8];
+                        int cell = -1;
                         if (in) {
                             X = axis32(x, dims.mx, dims.cx);
                             Y = axis32(y, dims.my, dims.cy);
                             Z = axis32(z, dims.mz, dims.cz);
                             corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+                            cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                         }
                         if (kPose) {
                             float value = 0.0f, gs[3] = {0.0f, 0.0f, 0.0f};
                             if (in) {
-                                float v[8];
-                                f.load(X.lower, Y.lower, Z.lower, v);
-                                value = interpolate(w, v);
+                                cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
+                                value = interpolate(w, cache.v);
                                 const float sx = (x >= 0.0f && x < dims.mx) ? 1.0f : 0.0f;
                                 const float sy = (y >= 0.0f && y < dims.my) ? 1.0f : 0.0f;
                                 const float sz = (z >= 0.0f && z < dims.mz) ? 1.0f : 0.0f;
-                                slope32(X.fraction, Y.fraction, Z.fraction, v, sx, sy, sz, gs);
+                                slope32(X.fraction, Y.fraction, Z.fraction, cache.v, sx, sy, sz, gs);
                             }
                             mean = mean + value;
 #pragma unroll
@@ -170,14 +172,13 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                                 dO[k] = dO[k] + gs[k];
                                 dD[k] = fmaf(position, gs[k], dD[k]);
                             }
-                            const float alpha = ((float)i + 0.5f) / (float)S;
+                            const float alpha = i < kAlphaTable ? alpha_table[i] : ((float)i + 0.5f) / (float)S;
                             const float along = fmaf(gs[2], d[2], fmaf(gs[1], d[1], gs[0] * d[0]));
                             sl = fmaf(1.0f - alpha, along, sl);
                             su = fmaf(alpha, along, su);
                         }
                         if (kVol) {
                             if (in) {
-                                const int cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                                 if (cell != pending) {
                                     if (pending >= 0) flush_cell(acc, pending, cs);
 #pragma unroll
@@ -186,8 +187,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                                 }
                                 if (bounded) {
 #pragma unroll
-                                    for (int c = 0; c < 8; ++c)
-                                        cs[c] = cs[c] + scatter_increment(vf, w[c]);
+                                    for (int c = 0; c < 8; ++c) cs[c] = cs[c] + mul_ftz(vf, w[c]);
                                 } else {
                                     float* slot = acc + 8 * (int64_t)cell;
 #pragma unroll
@@ -214,9 +214,21 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                                 pending = -1;
                             }
                         }
+                    };
+                    if (!moderate(o, d)) {
+                        for (int i = 0; i < S; ++i) visit(i, false);
+                    } else {
+                        // samples outside the inside run add exact zeros to every moment
+                        int first, last;
+                        inside_run(S, [&](int i) {
+                            const float position = position_at(i);
+                            return inside(fmaf(position, d[0], o[0]), fmaf(position, d[1], o[1]),
+                                          fmaf(position, d[2], o[2]), dims.hx, dims.hy, dims.hz);
+                        }, first, last);
+#pragma unroll 2
+                        for (int i = first; i <= last; ++i) visit(i, true);
                     }
                     if (kVol && pending >= 0) flush_cell(acc, pending, cs);
-                    if (!finite) bits |= 2;
                     if (kPose) {
                         float lo_o[3], lo_d[3], up_o[3], up_d[3];
                         iv.lower_gradients(lo_o, lo_d);
@@ -258,40 +270,57 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                     const double vf = factor * span / (double)S;
                     const bool power_of_two = (S & (S - 1)) == 0;
                     const double inverse_samples = power_of_two ? 1.0 / (double)S : 0.0;
+                    const double mx = (double)(dims.nx - 1), my = (double)(dims.ny - 1), mz = (double)(dims.nz - 1);
                     double mean = 0.0, dO[3] = {0.0, 0.0, 0.0}, dD[3] = {0.0, 0.0, 0.0};
                     double sl = 0.0, su = 0.0;
                     double cs[8];
 #pragma unroll
                     for (int c = 0; c < 8; ++c) cs[c] = 0.0;
                     int pending = -1;
-                    bool finite = true;
-                    for (int i = 0; i < S; ++i) {
-                        const double alpha = power_of_two ? ((double)i + 0.5) * inverse_samples
-                                                          : ((double)i + 0.5) / (double)S;
-                        const double position = fma((double)i + 0.5, step, iv.lower);
-                        double p[3];
+                    CellCache<Field> cache;
+                    auto flush64 = [&]() {
+                        float c32[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            c32[c] = (float)cs[c];
+                            cs[c] = 0.0;
+                        }
+                        flush_cell(acc, pending, c32);
+                    };
+                    auto point_at = [&](int i, double& position, double* p) {
+                        position = fma((double)i + 0.5, step, iv.lower);
 #pragma unroll
                         for (int k = 0; k < 3; ++k) p[k] = fma(position, r.direction[k], r.origin[k]);
-                        finite = finite && finite3(p[0], p[1], p[2]);
-                        const bool in = inside(p[0], p[1], p[2], dims.nx, dims.ny, dims.nz);
+                    };
+                    auto visit = [&](int i, bool known_inside) {
+                        const double alpha = power_of_two ? ((double)i + 0.5) * inverse_samples
+                                                          : ((double)i + 0.5) / (double)S;
+                        double position, p[3];
+                        point_at(i, position, p);
+                        bool in = true;
+                        if (!known_inside) {
+                            if (!finite3(p[0], p[1], p[2])) bits |= 2;
+                            in = inside(p[0], p[1], p[2], dims.nx, dims.ny, dims.nz);
+                        }
                         Axis64 X{0, 0.0}, Y{0, 0.0}, Z{0, 0.0};
+                        int cell = -1;
                         if (in) {
-                            X = axis64(p[0], (double)(dims.nx - 1), dims.cx);
-                            Y = axis64(p[1], (double)(dims.ny - 1), dims.cy);
-                            Z = axis64(p[2], (double)(dims.nz - 1), dims.cz);
+                            X = axis64(p[0], mx, dims.cx);
+                            Y = axis64(p[1], my, dims.cy);
+                            Z = axis64(p[2], mz, dims.cz);
+                            cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                         }
                         if (kPose) {
                             double value = 0.0, gs[3] = {0.0, 0.0, 0.0};
                             if (in) {
-                                float v32[8];
-                                f.load(X.lower, Y.lower, Z.lower, v32);
+                                cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
                                 double v[8];
 #pragma unroll
-                                for (int c = 0; c < 8; ++c) v[c] = (double)v32[c];
+                                for (int c = 0; c < 8; ++c) v[c] = (double)cache.v[c];
                                 value = interpolate64(X.fraction, Y.fraction, Z.fraction, v);
-                                const double sx = (p[0] >= 0.0 && p[0] < (double)(dims.nx - 1)) ? 1.0 : 0.0;
-                                const double sy = (p[1] >= 0.0 && p[1] < (double)(dims.ny - 1)) ? 1.0 : 0.0;
-                                const double sz = (p[2] >= 0.0 && p[2] < (double)(dims.nz - 1)) ? 1.0 : 0.0;
+                                const double sx = (p[0] >= 0.0 && p[0] < mx) ? 1.0 : 0.0;
+                                const double sy = (p[1] >= 0.0 && p[1] < my) ? 1.0 : 0.0;
+                                const double sz = (p[2] >= 0.0 && p[2] < mz) ? 1.0 : 0.0;
                                 slope64(X.fraction, Y.fraction, Z.fraction, v, sx, sy, sz, gs);
                             }
                             mean = mean + value;
@@ -307,16 +336,8 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                         }
                         if (kVol) {
                             if (in) {
-                                const int cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                                 if (cell != pending) {
-                                    if (pending >= 0) {
-                                        float c32[8];
-#pragma unroll
-                                        for (int c = 0; c < 8; ++c) c32[c] = (float)cs[c];
-                                        flush_cell(acc, pending, c32);
-                                    }
-#pragma unroll
-                                    for (int c = 0; c < 8; ++c) cs[c] = 0.0;
+                                    if (pending >= 0) flush64();
                                     pending = cell;
                                 }
                                 const double fx = X.fraction, fy = Y.fraction, fz = Z.fraction;
@@ -330,24 +351,23 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                                     cs[c] = cs[c] + (double)rounded;
                                 }
                             } else if (pending >= 0) {
-                                float c32[8];
-#pragma unroll
-                                for (int c = 0; c < 8; ++c) {
-                                    c32[c] = (float)cs[c];
-                                    cs[c] = 0.0;
-                                }
-                                flush_cell(acc, pending, c32);
+                                flush64();
                                 pending = -1;
                             }
                         }
+                    };
+                    if (!moderate(r.origin, r.direction)) {
+                        for (int i = 0; i < S; ++i) visit(i, false);
+                    } else {
+                        int first, last;
+                        inside_run(S, [&](int i) {
+                            double position, p[3];
+                            point_at(i, position, p);
+                            return inside(p[0], p[1], p[2], dims.nx, dims.ny, dims.nz);
+                        }, first, last);
+                        for (int i = first; i <= last; ++i) visit(i, true);
                     }
-                    if (kVol && pending >= 0) {
-                        float c32[8];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) c32[c] = (float)cs[c];
-                        flush_cell(acc, pending, c32);
-                    }
-                    if (!finite) bits |= 2;
+                    if (kVol && pending >= 0) flush64();
                     if (kPose) {
                         double lo_o[3], lo_d[3], up_o[3], up_d[3];
                         iv.lower_gradients(lo_o, lo_d);
@@ -400,38 +420,44 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
 #pragma unroll
                     for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                     int pending = -1;
-                    bool finite = true;
-#pragma unroll 2
-                    for (int i = 0; i < S; ++i) {
+                    CellCache<Field> cache;
+                    auto add_mean = [&](float value) {
+                        const float yk = value - carry;
+                        const float t = mean + yk;
+                        carry = (t - mean) - yk;
+                        mean = t;
+                    };
+                    auto visit = [&](int i, bool known_inside) {
                         const float offset = (float)i + 0.5f;
                         const float x = fmaf(offset, sv[0], entry[0]);
                         const float y = fmaf(offset, sv[1], entry[1]);
                         const float z = fmaf(offset, sv[2], entry[2]);
-                        finite = finite && finite3f(x, y, z);
-                        const bool in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                        bool in = true;
+                        if (!known_inside) {
+                            if (!finite3f(x, y, z)) bits |= 2;
+                            in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                        }
                         Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
                         float w[8];
+                        int cell = -1;
                         if (in) {
                             X = axis32(x, dims.mx, dims.cx);
                             Y = axis32(y, dims.my, dims.cy);
                             Z = axis32(z, dims.mz, dims.cz);
                             corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+                            cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                         }
                         if (kPose) {
                             float value = 0.0f, gs[3] = {0.0f, 0.0f, 0.0f};
                             if (in) {
-                                float v[8];
-                                f.load(X.lower, Y.lower, Z.lower, v);
-                                value = interpolate(w, v);
+                                cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
+                                value = interpolate(w, cache.v);
                                 const float sx = (x >= 0.0f && x < dims.mx) ? 1.0f : 0.0f;
                                 const float sy = (y >= 0.0f && y < dims.my) ? 1.0f : 0.0f;
                                 const float sz = (z >= 0.0f && z < dims.mz) ? 1.0f : 0.0f;
-                                slope32(X.fraction, Y.fraction, Z.fraction, v, sx, sy, sz, gs);
+                                slope32(X.fraction, Y.fraction, Z.fraction, cache.v, sx, sy, sz, gs);
                             }
-                            const float yk = value - carry;
-                            const float t = mean + yk;
-                            carry = (t - mean) - yk;
-                            mean = t;
+                            add_mean(value);
                             const float alpha = offset * inv_s;
 #pragma unroll
                             for (int k = 0; k < 3; ++k) {
@@ -441,7 +467,6 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                         }
                         if (kVol) {
                             if (in) {
-                                const int cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                                 if (cell != pending) {
                                     if (pending >= 0) flush_cell(acc, pending, cs);
 #pragma unroll
@@ -450,8 +475,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                                 }
                                 if (bounded) {
 #pragma unroll
-                                    for (int c = 0; c < 8; ++c)
-                                        cs[c] = cs[c] + scatter_increment(vf, w[c]);
+                                    for (int c = 0; c < 8; ++c) cs[c] = cs[c] + mul_ftz(vf, w[c]);
                                 } else {
                                     float* slot = acc + 8 * (int64_t)cell;
 #pragma unroll
@@ -468,9 +492,23 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                                 pending = -1;
                             }
                         }
+                    };
+                    if (!moderate(entry, sv)) {
+                        for (int i = 0; i < S; ++i) visit(i, false);
+                    } else {
+                        int first, last;
+                        inside_run(S, [&](int i) {
+                            const float offset = (float)i + 0.5f;
+                            return inside(fmaf(offset, sv[0], entry[0]), fmaf(offset, sv[1], entry[1]),
+                                          fmaf(offset, sv[2], entry[2]), dims.hx, dims.hy, dims.hz);
+                        }, first, last);
+#pragma unroll 2
+                        for (int i = first; i <= last; ++i) visit(i, true);
+                        // zero samples after the run still fold the compensation into the mean
+                        if (kPose)
+                            for (int i = max(last + 1, first); i < S; ++i) add_mean(0.0f);
                     }
                     if (kVol && pending >= 0) flush_cell(acc, pending, cs);
-                    if (!finite) bits |= 2;
                     if (kPose) {
                         const double* dr = r.direction;
                         const double Gd[3] = {G[0], G[1], G[2]}, Hd[3] = {H[0], H[1], H[2]};
