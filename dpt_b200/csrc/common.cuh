@@ -480,6 +480,101 @@ struct CellCache {
     }
 };
 
+// Axis coordinate of a point known to satisfy 0 <= p < n-1 (the interior of the grid): the
+// clamp and the cap of axis32 are then no-ops, so this is the same lower cell and fraction.
+__device__ __forceinline__ Axis32 interior_axis(float p)
+{
+    Axis32 r;
+    r.lower = __float2int_rd(p);
+    r.fraction = p - (float)r.lower;
+    return r;
+}
+
+// Interior run of the inside run: the samples whose point satisfies 0 <= p < n-1 on every
+// axis (all clamps inactive, all slope masks 1).  Also contiguous by monotonicity.
+template <typename Interior>
+__device__ __forceinline__ void interior_run(int first, int last, Interior interior_at, int& ifirst,
+                                             int& ilast)
+{
+    ifirst = first;
+    while (ifirst <= last && !interior_at(ifirst)) ++ifirst;
+    ilast = last;
+    while (ilast > ifirst && !interior_at(ilast)) --ilast;
+    if (ifirst > last) ilast = ifirst - 1;
+}
+
+// Trilinear polynomial of a cell, f = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz,
+// formed in FP32 from the eight corner values when a ray enters the cell (the arithmetic of
+// the compensated precision form).
+template <class Field>
+struct PolyCache {
+    float c[8];
+    int cell = -1;
+    __device__ __forceinline__ void fetch(const Field& f, int lx, int ly, int lz, int index)
+    {
+        if (index != cell) {
+            float v[8];
+            f.load(lx, ly, lz, v);
+            c[0] = v[0];
+            c[1] = v[1] - v[0];
+            c[2] = v[2] - v[0];
+            c[3] = v[4] - v[0];
+            c[4] = (v[3] - v[2]) - c[1];
+            c[5] = (v[5] - v[4]) - c[1];
+            c[6] = (v[6] - v[4]) - c[2];
+            c[7] = ((v[7] - v[6]) - (v[5] - v[4])) - c[4];
+            cell = index;
+        }
+    }
+    // value, and when `g` is given the derivatives d/dfx, d/dfy, d/dfz
+    __device__ __forceinline__ float eval(float fx, float fy, float fz, float* g = nullptr) const
+    {
+        const float a = fmaf(c[7], fz, c[4]), b = fmaf(c[5], fz, c[1]);
+        const float gx = fmaf(a, fy, b);
+        const float e = fmaf(c[6], fz, c[2]), h = fmaf(c[3], fz, c[0]);
+        if (g) {
+            g[0] = gx;
+            g[1] = fmaf(a, fx, e);
+            g[2] = fmaf(fx, fmaf(c[7], fy, c[5]), fmaf(c[6], fy, c[3]));
+        }
+        return fmaf(gx, fx, fmaf(e, fy, h));
+    }
+};
+
+// Compensated ray sum of the precision form: 16-sample blocks summed serially in FP32,
+// block sums added with Kahan compensation.  Blocks are aligned to the sample index.
+struct BlockSum {
+    float block = 0.0f, sum = 0.0f, carry = 0.0f;
+    __device__ __forceinline__ void kahan(float value)
+    {
+        const float y = value - carry;
+        const float t = sum + y;
+        carry = (t - sum) - y;
+        sum = t;
+    }
+    __device__ __forceinline__ void add(float value, int index, int samples)
+    {
+        block = block + value;
+        if ((index & 15) == 15 || index == samples - 1) {
+            kahan(block);
+            block = 0.0f;
+        }
+    }
+    // the blocks after sample `last` hold only zeros: close the open block, then add the
+    // zero block sums (which can still move the compensation into the sum)
+    __device__ __forceinline__ void finish(int last, int samples)
+    {
+        if (last >= samples - 1) return;  // the block of the last sample is already closed
+        if ((last & 15) != 15) {          // close the block containing `last`
+            kahan(block);
+            block = 0.0f;
+        }
+        // one zero sum per later block; once the compensation is zero they change nothing
+        for (int start = (last | 15) + 1; start < samples && carry != 0.0f; start += 16) kahan(0.0f);
+    }
+    __device__ __forceinline__ double value() const { return (double)sum - (double)carry; }
+};
+
 // FP32 product with results below the normal range flushed to signed zero: the scatter
 // increment of the reference (a rounded product, then |x| < 2^-126 -> 0, as CUDA's global
 // FP32 atomics treat subnormal operands), in one instruction.

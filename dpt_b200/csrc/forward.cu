@@ -10,8 +10,13 @@
 //          midpoints, fmaf corner sum, serial FP32 total, total *= length*step)
 //   F64  - python/dpt/kernels/projection.py:802-846 with the midpoint integrator 770-799
 //   F32C - FP64 setup and clip; FP32 marching p_i = entry + (i+0.5) step_vector (the mixed
-//          recurrence of python/dpt/kernels/projection.py:368-392), FP32 corner sum and a
-//          compensated FP32 ray sum scaled by length*step in FP64.
+//          recurrence of python/dpt/kernels/projection.py:368-392), FP32 samples from the
+//          cell's trilinear polynomial and a blocked compensated FP32 ray sum scaled by
+//          length*step in FP64 (the precision form of this build, no reference counterpart).
+//
+// Samples inside the support form one run; within it the interior run (0 <= p < n-1 on every
+// axis) skips the clamps of the cell coordinate.  Both are exact rewrites of the per-sample
+// tests, so every mode keeps its arithmetic bit for bit.
 #include "launch.h"
 
 namespace dpt {
@@ -106,18 +111,33 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                         at(i, x, y, z);
                         return inside(x, y, z, dims.hx, dims.hy, dims.hz);
                     }, first, last);
-                    CellCache<Field> cache;
-#pragma unroll 4
-                    for (int i = first; i <= last; ++i) {
+                    int ifirst, ilast;
+                    interior_run(first, last, [&](int i) {
                         float x, y, z;
                         at(i, x, y, z);
-                        const Axis32 X = axis32(x, dims.mx, dims.cx), Y = axis32(y, dims.my, dims.cy),
-                                     Z = axis32(z, dims.mz, dims.cz);
+                        return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
+                    }, ifirst, ilast);
+                    CellCache<Field> cache;
+                    auto add = [&](Axis32 X, Axis32 Y, Axis32 Z) {
                         cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
                         float w[8];
                         corner_weights(X.fraction, Y.fraction, Z.fraction, w);
                         total = total + interpolate(w, cache.v);
+                    };
+                    auto margin = [&](int i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        add(axis32(x, dims.mx, dims.cx), axis32(y, dims.my, dims.cy), axis32(z, dims.mz, dims.cz));
+                    };
+                    const int split = min(ifirst, last + 1);
+                    for (int i = first; i < split; ++i) margin(i);
+#pragma unroll 4
+                    for (int i = ifirst; i <= ilast; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        add(interior_axis(x), interior_axis(y), interior_axis(z));
                     }
+                    for (int i = max(ilast + 1, split); i <= last; ++i) margin(i);
                     // the zero samples after the run: adding +0 only turns -0 into +0
                     if (last < S - 1) total = total + 0.0f;
                 }
@@ -193,18 +213,25 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                     entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
                     sv[k] = (float)(step * r.direction[k]);
                 }
-                float sum = 0.0f, carry = 0.0f;
+                BlockSum acc;
                 auto at = [&](int i, float& x, float& y, float& z) {
                     const float offset = (float)i + 0.5f;
                     x = fmaf(offset, sv[0], entry[0]);
                     y = fmaf(offset, sv[1], entry[1]);
                     z = fmaf(offset, sv[2], entry[2]);
                 };
-                auto add = [&](float value) {
-                    const float yk = value - carry;
-                    const float t = sum + yk;
-                    carry = (t - sum) - yk;
-                    sum = t;
+                PolyCache<Field> cache;
+                auto add = [&](int i, Axis32 X, Axis32 Y, Axis32 Z) {
+                    cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
+                    acc.add(cache.eval(X.fraction, Y.fraction, Z.fraction), i, S);
+                };
+                auto margin = [&](int i) {
+                    float x, y, z;
+                    at(i, x, y, z);
+                    if (inside(x, y, z, dims.hx, dims.hy, dims.hz))
+                        add(i, axis32(x, dims.mx, dims.cx), axis32(y, dims.my, dims.cy), axis32(z, dims.mz, dims.cz));
+                    else
+                        acc.add(0.0f, i, S);
                 };
                 if (!moderate(entry, sv)) {
                     bool finite = true;
@@ -212,7 +239,7 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                         float x, y, z;
                         at(i, x, y, z);
                         finite = finite && finite3f(x, y, z);
-                        add(sample32(f, dims, x, y, z));
+                        margin(i);
                     }
                     if (!finite) bits |= 2;
                 } else {
@@ -222,22 +249,24 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                         at(i, x, y, z);
                         return inside(x, y, z, dims.hx, dims.hy, dims.hz);
                     }, first, last);
-                    CellCache<Field> cache;
-#pragma unroll 4
-                    for (int i = first; i <= last; ++i) {
+                    int ifirst, ilast;
+                    interior_run(first, last, [&](int i) {
                         float x, y, z;
                         at(i, x, y, z);
-                        const Axis32 X = axis32(x, dims.mx, dims.cx), Y = axis32(y, dims.my, dims.cy),
-                                     Z = axis32(z, dims.mz, dims.cz);
-                        cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
-                        float w[8];
-                        corner_weights(X.fraction, Y.fraction, Z.fraction, w);
-                        add(interpolate(w, cache.v));
+                        return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
+                    }, ifirst, ilast);
+                    const int split = min(ifirst, last + 1);
+                    for (int i = first; i < split; ++i) margin(i);
+#pragma unroll 4
+                    for (int i = ifirst; i <= ilast; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        add(i, interior_axis(x), interior_axis(y), interior_axis(z));
                     }
-                    // zero samples after the run still move the compensation into the sum
-                    for (int i = max(last + 1, first); i < S; ++i) add(0.0f);
+                    for (int i = max(ilast + 1, split); i <= last; ++i) margin(i);
+                    acc.finish(max(last, first - 1), S);
                 }
-                result = ((double)sum - (double)carry) * (r.length * step);
+                result = acc.value() * (r.length * step);
             }
             if (!finite_out<Out>(result)) bits |= 2;
         }

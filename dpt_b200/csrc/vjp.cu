@@ -134,9 +134,11 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                     int pending = -1;
                     CellCache<Field> cache;
                     auto position_at = [&](int i) { return fmaf((float)i + 0.5f, step, iv.lower); };
-                    // One midpoint; `known_inside` is true on the inside run, where the support
-                    // and finiteness tests are known to pass.
-                    auto visit = [&](int i, bool known_inside) {
+                    // One midpoint.  mode 0: general (support and finiteness tested); 1: on the
+                    // inside run (both known to pass); 2: on the interior run (no clamp active,
+                    // slope masks 1).
+                    auto visit = [&](int i, int mode) {
+                        const bool known_inside = mode > 0;
                         const float position = position_at(i);
                         const float x = fmaf(position, d[0], o[0]);
                         const float y = fmaf(position, d[1], o[1]);
@@ -149,10 +151,16 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                         Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
                         float w[8];
                         int cell = -1;
-                        if (in) {
+                        if (mode == 2) {
+                            X = interior_axis(x);
+                            Y = interior_axis(y);
+                            Z = interior_axis(z);
+                        } else if (in) {
                             X = axis32(x, dims.mx, dims.cx);
                             Y = axis32(y, dims.my, dims.cy);
                             Z = axis32(z, dims.mz, dims.cz);
+                        }
+                        if (in) {
                             corner_weights(X.fraction, Y.fraction, Z.fraction, w);
                             cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                         }
@@ -161,9 +169,10 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                             if (in) {
                                 cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
                                 value = interpolate(w, cache.v);
-                                const float sx = (x >= 0.0f && x < dims.mx) ? 1.0f : 0.0f;
-                                const float sy = (y >= 0.0f && y < dims.my) ? 1.0f : 0.0f;
-                                const float sz = (z >= 0.0f && z < dims.mz) ? 1.0f : 0.0f;
+                                const bool core = mode == 2;
+                                const float sx = (core || (x >= 0.0f && x < dims.mx)) ? 1.0f : 0.0f;
+                                const float sy = (core || (y >= 0.0f && y < dims.my)) ? 1.0f : 0.0f;
+                                const float sz = (core || (z >= 0.0f && z < dims.mz)) ? 1.0f : 0.0f;
                                 slope32(X.fraction, Y.fraction, Z.fraction, cache.v, sx, sy, sz, gs);
                             }
                             mean = mean + value;
@@ -216,7 +225,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                         }
                     };
                     if (!moderate(o, d)) {
-                        for (int i = 0; i < S; ++i) visit(i, false);
+                        for (int i = 0; i < S; ++i) visit(i, 0);
                     } else {
                         // samples outside the inside run add exact zeros to every moment
                         int first, last;
@@ -225,8 +234,18 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                             return inside(fmaf(position, d[0], o[0]), fmaf(position, d[1], o[1]),
                                           fmaf(position, d[2], o[2]), dims.hx, dims.hy, dims.hz);
                         }, first, last);
+                        int ifirst, ilast;
+                        interior_run(first, last, [&](int i) {
+                            const float position = position_at(i);
+                            const float x = fmaf(position, d[0], o[0]), y = fmaf(position, d[1], o[1]),
+                                        z = fmaf(position, d[2], o[2]);
+                            return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
+                        }, ifirst, ilast);
+                        const int split = min(ifirst, last + 1);
+                        for (int i = first; i < split; ++i) visit(i, 1);
 #pragma unroll 2
-                        for (int i = first; i <= last; ++i) visit(i, true);
+                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2);
+                        for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1);
                     }
                     if (kVol && pending >= 0) flush_cell(acc, pending, cs);
                     if (kPose) {
@@ -394,8 +413,10 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                 }
             }
         } else {
-            // F32C: FP64 clip, FP32 marching and sample arithmetic, pose moments
-            // G = sum grad and H = sum alpha grad with the integral, chained in FP64.
+            // F32C: FP64 clip; FP32 marching; value and slope from the cell's trilinear
+            // polynomial; blocked compensated mean; pose moments G = sum grad, H = sum alpha
+            // grad; volume scatter through per-run moments of the fractions, expanded into
+            // the eight corner sums at the end of each cell run.
             if (!valid_ray(r)) {
                 bits = 2;
             } else {
@@ -407,7 +428,6 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                 if (span > 0.0 && seed != 0.0) {
                     const double step = span / (double)S;
                     const float vf = (float)(seed * r.length * step);
-                    const bool bounded = isfinite(vf) && fabsf(vf) <= 1.0f;
                     float entry[3], sv[3];
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
@@ -415,50 +435,73 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                         sv[k] = (float)(step * r.direction[k]);
                     }
                     const float inv_s = 1.0f / (float)S;
-                    float mean = 0.0f, carry = 0.0f, G[3] = {0.0f, 0.0f, 0.0f}, H[3] = {0.0f, 0.0f, 0.0f};
-                    float cs[8];
+                    BlockSum mean;
+                    float G[3] = {0.0f, 0.0f, 0.0f}, H[3] = {0.0f, 0.0f, 0.0f};
+                    float m[8];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                    for (int c = 0; c < 8; ++c) m[c] = 0.0f;
                     int pending = -1;
-                    CellCache<Field> cache;
-                    auto add_mean = [&](float value) {
-                        const float yk = value - carry;
-                        const float t = mean + yk;
-                        carry = (t - mean) - yk;
-                        mean = t;
+                    PolyCache<Field> cache;
+                    auto flush = [&]() {
+                        float corner[8];
+                        corner[7] = m[7];
+                        corner[3] = m[4] - m[7];
+                        corner[5] = m[5] - m[7];
+                        corner[6] = m[6] - m[7];
+                        corner[1] = (m[1] - m[4]) - corner[5];
+                        corner[2] = (m[2] - m[4]) - corner[6];
+                        corner[4] = (m[3] - m[5]) - corner[6];
+                        corner[0] = ((m[0] - m[1]) - (m[2] - m[4])) - corner[4];
+                        bool finite = true;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            corner[c] = vf * corner[c];
+                            finite = finite && isfinite(corner[c]);
+                            m[c] = 0.0f;
+                        }
+                        if (!finite) bits |= 2;
+                        flush_cell(acc, pending, corner);
                     };
-                    auto visit = [&](int i, bool known_inside) {
+                    auto point_at = [&](int i, float& x, float& y, float& z) {
                         const float offset = (float)i + 0.5f;
-                        const float x = fmaf(offset, sv[0], entry[0]);
-                        const float y = fmaf(offset, sv[1], entry[1]);
-                        const float z = fmaf(offset, sv[2], entry[2]);
+                        x = fmaf(offset, sv[0], entry[0]);
+                        y = fmaf(offset, sv[1], entry[1]);
+                        z = fmaf(offset, sv[2], entry[2]);
+                    };
+                    // mode 0: general; 1: inside run; 2: interior run
+                    auto visit = [&](int i, int mode) {
+                        float x, y, z;
+                        point_at(i, x, y, z);
                         bool in = true;
-                        if (!known_inside) {
+                        if (mode == 0) {
                             if (!finite3f(x, y, z)) bits |= 2;
                             in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
                         }
                         Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
-                        float w[8];
                         int cell = -1;
-                        if (in) {
+                        if (mode == 2) {
+                            X = interior_axis(x);
+                            Y = interior_axis(y);
+                            Z = interior_axis(z);
+                        } else if (in) {
                             X = axis32(x, dims.mx, dims.cx);
                             Y = axis32(y, dims.my, dims.cy);
                             Z = axis32(z, dims.mz, dims.cz);
-                            corner_weights(X.fraction, Y.fraction, Z.fraction, w);
-                            cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                         }
+                        if (in) cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                         if (kPose) {
                             float value = 0.0f, gs[3] = {0.0f, 0.0f, 0.0f};
                             if (in) {
                                 cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
-                                value = interpolate(w, cache.v);
-                                const float sx = (x >= 0.0f && x < dims.mx) ? 1.0f : 0.0f;
-                                const float sy = (y >= 0.0f && y < dims.my) ? 1.0f : 0.0f;
-                                const float sz = (z >= 0.0f && z < dims.mz) ? 1.0f : 0.0f;
-                                slope32(X.fraction, Y.fraction, Z.fraction, cache.v, sx, sy, sz, gs);
+                                value = cache.eval(X.fraction, Y.fraction, Z.fraction, gs);
+                                if (mode != 2) {
+                                    if (!(x >= 0.0f && x < dims.mx)) gs[0] = 0.0f * gs[0];
+                                    if (!(y >= 0.0f && y < dims.my)) gs[1] = 0.0f * gs[1];
+                                    if (!(z >= 0.0f && z < dims.mz)) gs[2] = 0.0f * gs[2];
+                                }
                             }
-                            add_mean(value);
-                            const float alpha = offset * inv_s;
+                            mean.add(value, i, S);
+                            const float alpha = ((float)i + 0.5f) * inv_s;
 #pragma unroll
                             for (int k = 0; k < 3; ++k) {
                                 G[k] = G[k] + gs[k];
@@ -468,51 +511,52 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                         if (kVol) {
                             if (in) {
                                 if (cell != pending) {
-                                    if (pending >= 0) flush_cell(acc, pending, cs);
-#pragma unroll
-                                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                                    if (pending >= 0) flush();
                                     pending = cell;
                                 }
-                                if (bounded) {
-#pragma unroll
-                                    for (int c = 0; c < 8; ++c) cs[c] = cs[c] + mul_ftz(vf, w[c]);
-                                } else {
-                                    float* slot = acc + 8 * (int64_t)cell;
-#pragma unroll
-                                    for (int c = 0; c < 8; ++c) {
-                                        const float inc = scatter_increment(vf, w[c]);
-                                        if (!isfinite(inc)) bits |= 2;
-                                        atomicAdd(slot + c, inc);
-                                    }
-                                }
+                                const float fx = X.fraction, fy = Y.fraction, fz = Z.fraction;
+                                const float fxy = fx * fy;
+                                m[0] = m[0] + 1.0f;
+                                m[1] = m[1] + fx;
+                                m[2] = m[2] + fy;
+                                m[3] = m[3] + fz;
+                                m[4] = m[4] + fxy;
+                                m[5] = m[5] + fx * fz;
+                                m[6] = m[6] + fy * fz;
+                                m[7] = m[7] + fxy * fz;
                             } else if (pending >= 0) {
-                                flush_cell(acc, pending, cs);
-#pragma unroll
-                                for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                                flush();
                                 pending = -1;
                             }
                         }
                     };
                     if (!moderate(entry, sv)) {
-                        for (int i = 0; i < S; ++i) visit(i, false);
+                        for (int i = 0; i < S; ++i) visit(i, 0);
                     } else {
                         int first, last;
                         inside_run(S, [&](int i) {
-                            const float offset = (float)i + 0.5f;
-                            return inside(fmaf(offset, sv[0], entry[0]), fmaf(offset, sv[1], entry[1]),
-                                          fmaf(offset, sv[2], entry[2]), dims.hx, dims.hy, dims.hz);
+                            float x, y, z;
+                            point_at(i, x, y, z);
+                            return inside(x, y, z, dims.hx, dims.hy, dims.hz);
                         }, first, last);
+                        int ifirst, ilast;
+                        interior_run(first, last, [&](int i) {
+                            float x, y, z;
+                            point_at(i, x, y, z);
+                            return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
+                        }, ifirst, ilast);
+                        const int split = min(ifirst, last + 1);
+                        for (int i = first; i < split; ++i) visit(i, 1);
 #pragma unroll 2
-                        for (int i = first; i <= last; ++i) visit(i, true);
-                        // zero samples after the run still fold the compensation into the mean
-                        if (kPose)
-                            for (int i = max(last + 1, first); i < S; ++i) add_mean(0.0f);
+                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2);
+                        for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1);
+                        if (kPose) mean.finish(max(last, first - 1), S);
                     }
-                    if (kVol && pending >= 0) flush_cell(acc, pending, cs);
+                    if (kVol && pending >= 0) flush();
                     if (kPose) {
                         const double* dr = r.direction;
                         const double Gd[3] = {G[0], G[1], G[2]}, Hd[3] = {H[0], H[1], H[2]};
-                        const double mean64 = (double)mean - (double)carry;
+                        const double mean64 = mean.value();
                         const double g_along = fma(Gd[2], dr[2], fma(Gd[1], dr[1], Gd[0] * dr[0]));
                         const double h_along = fma(Hd[2], dr[2], fma(Hd[1], dr[1], Hd[0] * dr[0]));
                         const double su = h_along, sl = g_along - h_along;

@@ -229,25 +229,49 @@ def chest_phantom(grid: GridSpec, *, seed: int = 0) -> np.ndarray:
 
 
 def head_phantom(grid: GridSpec, *, seed: int = 0) -> np.ndarray:
-    """Head-like attenuation volume: 6 mm skull shell (+1000 HU), brain 30 +- 10 HU,
-    two ventricles (5 HU), air outside; 60 keV water model, FP32 mm^-1."""
+    """Head-like attenuation volume in RAS object coordinates (x right, y anterior,
+    z superior): a skull shell (+1000 HU; 6 mm, 10 mm over the occiput), brain
+    30 +- 10 HU, two ventricles (5 HU), a calcified pineal spot (+400 HU, off the
+    midline), two orbits (fat, -100 HU) and a frontal sinus (air) cut into the
+    anterior skull, two petrous ridges (+1500 HU) and a mandible arc (+1800 HU)
+    below; air outside; 60 keV water model, FP32 mm^-1.  The anterior and inferior
+    structures break the shell's symmetries so that every rotation is observable
+    from two orthogonal views."""
     rng = np.random.default_rng(seed)
     nz, ny, nx = grid.shape
     centre = grid.grid_to_object(((nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2))
     extent = (nx * grid.spacing_mm[0], ny * grid.spacing_mm[1], nz * grid.spacing_mm[2])
-    outer = (0.42 * extent[0], 0.46 * extent[1], 0.46 * extent[2])
+    ex, ey, ez = extent
+    outer = (0.42 * ex, 0.46 * ey, 0.46 * ez)
     inner = tuple(a - 6.0 for a in outer)
-    ventricles = ((-0.06 * extent[0], 0.0, 0.0), (0.06 * extent[0], 0.0, 0.0))
-    ventricle_axes = (0.04 * extent[0], 0.12 * extent[1], 0.15 * extent[2])
+    occiput = (0.0, -0.10 * ey, 0.0)
+    occiput_axes = (outer[0] - 10.0, outer[1] - 4.0, outer[2] - 10.0)
+    ventricles = ((-0.06 * ex, 0.0, 0.0), (0.06 * ex, 0.0, 0.0))
+    ventricle_axes = (0.04 * ex, 0.12 * ey, 0.15 * ez)
+    pineal = ((0.03 * ex, -0.08 * ey, 0.05 * ez), (0.015 * ex, 0.015 * ey, 0.02 * ez))
+    orbits = (((-0.13 * ex, 0.38 * ey, -0.08 * ez), (0.07 * ex, 0.08 * ey, 0.09 * ez)),
+              ((0.13 * ex, 0.38 * ey, -0.08 * ez), (0.07 * ex, 0.08 * ey, 0.09 * ez)))
+    sinus = ((0.01 * ex, 0.40 * ey, 0.12 * ez), (0.10 * ex, 0.05 * ey, 0.07 * ez))
+    petrous = (((-0.22 * ex, -0.05 * ey, -0.25 * ez), (0.14 * ex, 0.03 * ey, 0.04 * ez)),
+               ((0.22 * ex, -0.05 * ey, -0.25 * ez), (0.14 * ex, 0.03 * ey, 0.04 * ez)))
+    jaw_outer = ((0.0, 0.22 * ey, -0.40 * ez), (0.30 * ex, 0.22 * ey, 0.06 * ez))
+    jaw_inner = ((0.0, 0.16 * ey, -0.40 * ez), (0.25 * ex, 0.18 * ey, 0.07 * ez))
     out = np.empty(grid.shape, dtype=np.float32)
     for z in range(nz):
         coords = [c - centre[k] for k, c in enumerate(_object_coordinates(grid, z))]
         hu = np.full(coords[0].shape, -1000.0)
         skull = _ellipse_mask(coords, (0.0, 0.0, 0.0), outer)
-        brain = _ellipse_mask(coords, (0.0, 0.0, 0.0), inner)
+        brain = _ellipse_mask(coords, (0.0, 0.0, 0.0), inner) & _ellipse_mask(coords, occiput, occiput_axes)
         hu[skull] = 1000.0
         hu[brain] = rng.normal(30.0, 10.0, int(brain.sum()))
         for c in ventricles:
             hu[_ellipse_mask(coords, c, ventricle_axes) & brain] = 5.0
+        hu[_ellipse_mask(coords, *pineal) & brain] = 400.0
+        for c, axes in orbits:
+            hu[_ellipse_mask(coords, c, axes)] = -100.0
+        hu[_ellipse_mask(coords, *sinus)] = -1000.0
+        for c, axes in petrous:
+            hu[_ellipse_mask(coords, c, axes)] = 1500.0
+        hu[_ellipse_mask(coords, *jaw_outer) & ~_ellipse_mask(coords, *jaw_inner)] = 1800.0
         out[z] = hu_to_mu(hu)
     return out

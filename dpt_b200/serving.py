@@ -179,14 +179,25 @@ class _Job:
 
 
 class _Slot:
-    """One CUDA stream with its own workspaces (scratch is never shared across slots)."""
+    """One CUDA stream with its own workspaces (scratch is never shared across slots) and
+    reusable pinned staging buffers (a slot runs one request at a time)."""
 
-    def __init__(self, torch, device, index: int) -> None:
+    def __init__(self, torch, device, index: int, stream=None) -> None:
+        self.torch = torch
         self.index = index
-        self.stream = torch.cuda.Stream(device=device)
+        self.stream = torch.cuda.Stream(device=device) if stream is None else stream
         self.workspaces: OrderedDict[Any, Any] = OrderedDict()
         self.graphs: dict[Any, Any] = {}
         self.busy = False
+        self._pinned: dict[str, Any] = {}
+
+    def pinned(self, name: str, count: int, dtype):
+        """A pinned host buffer of at least ``count`` elements, reused across requests."""
+        buffer = self._pinned.get(name)
+        if buffer is None or buffer.numel() < count or buffer.dtype != dtype:
+            buffer = self.torch.empty(max(count, 64), dtype=dtype, pin_memory=True)
+            self._pinned[name] = buffer
+        return buffer[:count]
 
 
 class ProjectionServer:
@@ -216,6 +227,8 @@ class ProjectionServer:
         self.autotune = autotune
         self.workspaces_per_slot = workspaces_per_slot
         self.volumes: dict[str, _Volume] = {}
+        self._alone: _Slot | None = None
+        self._identity: dict[int, Any] = {}
         self.lock = threading.Condition()
         self.inbox: queue.Queue = queue.Queue()
         self.running: deque[_Job] = deque()
@@ -262,14 +275,15 @@ class ProjectionServer:
         return future
 
     def run_alone(self, request: ProjectionRequest) -> ProjectionResult:
-        """Run one request synchronously on the caller's stream (the sequential baseline)."""
+        """Run one request synchronously on the caller's stream (the sequential baseline:
+        plain calls with their workspaces kept warm, no graphs, no tuning)."""
+        if self._alone is None:
+            self._alone = _Slot(self.torch, self.device, -1, self.torch.cuda.current_stream(self.device))
         job = _Job(request, Future(), time.perf_counter())
-        slot = _Slot(self.torch, self.device, -1)
-        slot.stream = self.torch.cuda.current_stream(self.device)
-        job.slot = slot
+        job.slot = self._alone
         job.started = time.perf_counter()
         self._launch(job, use_graph=False)
-        self.torch.cuda.current_stream(self.device).synchronize()
+        job.event.synchronize()
         return self._finish(job)
 
     def close(self) -> None:
@@ -339,9 +353,12 @@ class ProjectionServer:
                     self.lock.wait(0.05)
                 if not self.running:
                     return
-                job = self.running.popleft()
-            if job.event is not None:
-                job.event.synchronize()
+                # complete whichever request finished first: no head-of-line blocking
+                job = next((j for j in self.running if j.event is None or j.event.query()), None)
+                if job is None:
+                    self.lock.wait(0.0002)
+                    continue
+                self.running.remove(job)
             try:
                 if "error" in job.outputs:
                     raise job.outputs["error"]
@@ -384,19 +401,29 @@ class ProjectionServer:
             slot.workspaces.move_to_end(key)
         return key, found
 
-    def _poses(self, request: ProjectionRequest, views: int):
+    def _poses(self, request: ProjectionRequest, views: int, slot: _Slot | None = None):
+        """Device poses ``(views, 12)``: a cached identity, or the composed tangent staged
+        through the slot's pinned buffer."""
         import numpy as np
 
         from .geometry import RigidTransform, compose_pose
 
+        torch = self.torch
         if request.tangent is None:
-            packed = np.tile(np.asarray(RigidTransform().packed()), (views, 1))
-        else:
-            tangent = np.asarray(request.tangent, dtype=np.float64).reshape(-1, 6)
-            tangent = np.broadcast_to(tangent, (views, 6))
-            packed = np.asarray([compose_pose(RigidTransform(), tuple(map(float, t))).packed()
-                                 for t in tangent])
-        return self.torch.tensor(packed, dtype=self.torch.float64)
+            found = self._identity.get(views)
+            if found is None:
+                identity = torch.tensor(RigidTransform().packed(), dtype=torch.float64, device=self.device)
+                found = identity.expand(views, 12).contiguous()
+                self._identity[views] = found
+            return found
+        tangent = np.asarray(request.tangent, dtype=np.float64).reshape(-1, 6)
+        tangent = np.broadcast_to(tangent, (views, 6))
+        packed = np.asarray([compose_pose(RigidTransform(), tuple(map(float, t))).packed() for t in tangent])
+        if slot is None:
+            return torch.tensor(packed, dtype=torch.float64, device=self.device)
+        host = slot.pinned("poses", views * 12, torch.float64)
+        host.copy_(torch.from_numpy(packed.reshape(-1)))
+        return host.view(views, 12).to(self.device, non_blocking=True)
 
     def _block_cols(self, request: ProjectionRequest, slot: _Slot) -> int:
         from .plan import batched
@@ -411,7 +438,7 @@ class ProjectionServer:
 
         def run(cols: int) -> float:
             _, ws = self._workspace(slot, request, cols)
-            poses = self._poses(request, len(geometry.views)).to(self.device)
+            poses = self._poses(request, len(geometry.views))
             with torch.cuda.stream(slot.stream):
                 ws.forward(volume.field, poses, checked=False)  # warm
                 start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -432,25 +459,20 @@ class ProjectionServer:
         volume = self.volumes[request.volume]
         views = ws.plan.views
         with torch.cuda.stream(slot.stream):
-            poses_host = self._poses(request, views).pin_memory()
-            target = request.target
             state = slot.graphs.get(key) if use_graph else None
             if state is None:
-                inputs = {"poses": poses_host.to(self.device, non_blocking=True),
-                          "target": self._target(request, ws)}
+                inputs = {"poses": self._poses(request, views, slot), "target": self._target(request, ws)}
                 outputs = self._body(ws, volume.field, inputs, request)
                 if use_graph:
                     self._capture(slot, key, ws, volume.field, request, inputs)
             else:
                 graph, inputs, outputs = state
-                inputs["poses"].copy_(poses_host, non_blocking=True)
-                if target is not None:
-                    inputs["target"].copy_(self._as_device(target), non_blocking=True)
-                else:
-                    inputs["target"].zero_()
+                inputs["poses"].copy_(self._poses(request, views, slot), non_blocking=True)
+                if inputs["target"] is not None:
+                    inputs["target"].copy_(self._target(request, ws), non_blocking=True)
                 graph.replay()
                 outputs = {name: value.clone() for name, value in outputs.items()}
-            status_host = torch.empty(views, dtype=torch.int32, pin_memory=True)
+            status_host = slot.pinned("status", views, torch.int32)
             status_host.copy_(ws.status, non_blocking=True)
             ws.status.zero_()
             job.outputs = dict(outputs, status=status_host)
@@ -464,9 +486,9 @@ class ProjectionServer:
         return tensor.to(self.device, non_blocking=True)
 
     def _target(self, request: ProjectionRequest, ws):
-        torch = self.torch
-        if request.target is None:
-            return torch.zeros(ws.plan.image_shape, dtype=ws.spec.image_dtype, device=self.device)
+        """Device target image, or None for a zero target (the residual is then the image)."""
+        if request.kind == "forward" or request.target is None:
+            return None
         return self._as_device(request.target).to(ws.spec.image_dtype).reshape(ws.plan.image_shape).clone()
 
     def _body(self, ws, field_tensor, inputs, request: ProjectionRequest) -> dict:
@@ -474,7 +496,7 @@ class ProjectionServer:
         image = ws.forward(field_tensor, inputs["poses"], checked=False)
         out = {"image": image}
         if request.kind != "forward":
-            residual = image - inputs["target"]
+            residual = image if inputs["target"] is None else image - inputs["target"]
             out["loss"] = 0.5 * (residual.double() * residual.double()).sum()
             if request.kind == "volume":
                 out["volume_gradient"], _ = ws.vjp(field_tensor, inputs["poses"], residual, volume=True,
@@ -486,7 +508,8 @@ class ProjectionServer:
 
     def _capture(self, slot: _Slot, key, ws, field_tensor, request, inputs) -> None:
         torch = self.torch
-        static = {"poses": inputs["poses"].clone(), "target": inputs["target"].clone()}
+        static = {"poses": inputs["poses"].clone(),
+                  "target": None if inputs["target"] is None else inputs["target"].clone()}
         graph = torch.cuda.CUDAGraph()
         slot.stream.synchronize()
         with torch.cuda.graph(graph, stream=slot.stream):

@@ -29,9 +29,10 @@
  * a + b*c it uses fma(b, c, a).  The CUDA kernels follow the same contract, so
  * forward images, clip intervals and sample counts agree bit for bit.
  *
- * The DPT_ARITH_F32C form (FP64 clip, FP32 marching, compensated sum) has no
- * reference counterpart: it is the storage-precision form of this build and is
- * checked here against its own definition and, in the tests, against F64.
+ * The DPT_ARITH_F32C form (FP64 clip, FP32 marching, trilinear-polynomial samples,
+ * blocked compensated sum, moment-based scatter) has no reference counterpart: it is
+ * the storage-precision form of this build, restated here from its own definition
+ * and checked in the tests against F64.
  */
 #include <math.h>
 #include <stdint.h>
@@ -402,6 +403,53 @@ static double sample64(const dpt_problem* p, const void* field, const double* q,
     return value;
 }
 
+/* F32C sample: value and grid slope from the trilinear polynomial of the cell,
+ * f = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz, coefficients formed in FP32
+ * from the eight corners in the order below and evaluated with fmaf. */
+static float sample32c(const dpt_problem* p, const void* field, const float* q, const int* shape,
+                       float* gradient, float* fraction_out)
+{
+    if (gradient) gradient[0] = gradient[1] = gradient[2] = 0.0f;
+    if (!inside32(q, shape)) return 0.0f;
+    int lower[3];
+    float f[3], slope[3], v[8];
+    coordinates32(q, shape, lower, f, slope);
+    if (fraction_out) memcpy(fraction_out, f, sizeof(f));
+    for (int c = 0; c < 8; ++c) v[c] = field_value(p, field, corner_index(lower, shape, c));
+    const float c0 = v[0], c1 = v[1] - v[0], c2 = v[2] - v[0], c3 = v[4] - v[0];
+    const float c4 = (v[3] - v[2]) - c1, c5 = (v[5] - v[4]) - c1, c6 = (v[6] - v[4]) - c2;
+    const float c7 = ((v[7] - v[6]) - (v[5] - v[4])) - c4;
+    const float fx = f[0], fy = f[1], fz = f[2];
+    const float a = fmaf(c7, fz, c4), b = fmaf(c5, fz, c1);
+    const float gx = fmaf(a, fy, b);
+    const float e = fmaf(c6, fz, c2), h = fmaf(c3, fz, c0);
+    const float value = fmaf(gx, fx, fmaf(e, fy, h));
+    if (gradient) {
+        gradient[0] = slope[0] * gx;
+        gradient[1] = slope[1] * fmaf(a, fx, e);
+        gradient[2] = slope[2] * fmaf(fx, fmaf(c7, fy, c5), fmaf(c6, fy, c3));
+    }
+    return value;
+}
+
+/* Compensated sum of 16-sample blocks: each block summed serially in FP32, the block sums
+ * added with Kahan compensation. */
+typedef struct {
+    float block, sum, carry;
+} blocksum_t;
+
+static void blocksum_add(blocksum_t* s, float value, int index, int samples)
+{
+    s->block += value;
+    if ((index & 15) == 15 || index == samples - 1) {
+        float y = s->block - s->carry;
+        float t = s->sum + y;
+        s->carry = (t - s->sum) - y;
+        s->sum = t;
+        s->block = 0.0f;
+    }
+}
+
 /* ------------------------------------------------------------ ray geometry */
 
 typedef struct {
@@ -495,23 +543,21 @@ static int forward_ray(const dpt_problem* p, const void* field, const ray_t* ray
         *out = integral;
         if (!isfinite(p->image_dtype == DPT_F32 ? (double)(float)integral : integral)) status |= 2;
     } else {
-        /* F32C: FP32 samples with a compensated sum, FP64 scale. */
+        /* F32C: FP32 polynomial samples, blocked compensated sum, FP64 scale. */
         const interval64_t* iv = &ray->iv64;
         double integral = 0.0;
         if (iv->upper > iv->lower) {
-            float entry[3], stepv[3], sum = 0.0f, carry = 0.0f;
+            float entry[3], stepv[3];
+            blocksum_t acc = {0.0f, 0.0f, 0.0f};
             march32c(ray, S, entry, stepv);
             for (int i = 0; i < S; ++i) {
                 float q[3];
                 point32c(entry, stepv, i, q);
                 if (!finite3f(q)) status |= 2;
-                float y = sample32(p, field, q, shape, NULL) - carry;
-                float t = sum + y;
-                carry = (t - sum) - y;
-                sum = t;
+                blocksum_add(&acc, sample32c(p, field, q, shape, NULL, NULL), i, S);
             }
             double step = (iv->upper - iv->lower) / (double)S;
-            integral = ((double)sum - (double)carry) * (ray->r.length * step);
+            integral = ((double)acc.sum - (double)acc.carry) * (ray->r.length * step);
         }
         *out = integral;
         if (!isfinite(p->image_dtype == DPT_F32 ? (double)(float)integral : integral)) status |= 2;
@@ -896,8 +942,39 @@ static int vjp_ray_f64(const dpt_problem* p, const void* field, const ray_t* ray
     return status;
 }
 
-/* One ray of the F32C VJP: FP64 clip and clip-face chain, FP32 marching and sample
- * arithmetic, pose moments G = sum grad, H = sum alpha grad and the integral sum. */
+/* F32C volume scatter: per run of samples in one cell, FP32 moments of the fractions
+ * (count, fx, fy, fz, fx fy, fx fz, fy fz, fx fy fz) expand at the end of the run into the
+ * eight corner weight sums, which are scaled by the ray's factor once. */
+typedef struct {
+    int pending[3];
+    float m[8];
+} moments_t;
+
+static int flush_moments(const dpt_problem* p, moments_t* mo, float factor, double* gradient)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0;
+    const float* m = mo->m;
+    float corner[8];
+    corner[7] = m[7];
+    corner[3] = m[4] - m[7];
+    corner[5] = m[5] - m[7];
+    corner[6] = m[6] - m[7];
+    corner[1] = (m[1] - m[4]) - corner[5];
+    corner[2] = (m[2] - m[4]) - corner[6];
+    corner[4] = (m[3] - m[5]) - corner[6];
+    corner[0] = ((m[0] - m[1]) - (m[2] - m[4])) - corner[4];
+    for (int c = 0; c < 8; ++c) {
+        float increment = factor * corner[c];
+        if (!isfinite(increment)) status |= 2;
+        gradient[corner_index(mo->pending, shape, c)] += (double)increment;
+    }
+    memset(mo->m, 0, sizeof(mo->m));
+    return status;
+}
+
+/* One ray of the F32C VJP: FP64 clip and clip-face chain, FP32 marching, polynomial
+ * values and slopes, blocked compensated mean, pose moments G = sum grad and
+ * H = sum alpha grad, moment-based volume scatter. */
 static int vjp_ray_f32c(const dpt_problem* p, const void* field, const ray_t* ray, double seed,
                         int flags, scatter_t* sc, double* g12, double* g6)
 {
@@ -910,23 +987,22 @@ static int vjp_ray_f32c(const dpt_problem* p, const void* field, const ray_t* ra
     if (!(span > 0.0 && seed != 0.0)) return status;
     double step = span / (double)S;
     float volume_factor = (float)(seed * ray->r.length * step);
-    int bounded = isfinite(volume_factor) && fabsf(volume_factor) <= 1.0f;
     float entry[3], stepv[3];
     march32c(ray, S, entry, stepv);
-    float mean = 0.0f, mean_carry = 0.0f, G[3] = {0}, H[3] = {0};
+    blocksum_t mean = {0.0f, 0.0f, 0.0f};
+    float G[3] = {0}, H[3] = {0};
     float inv_s = 1.0f / (float)S;
-    sc->pending[0] = sc->pending[1] = sc->pending[2] = -1;
-    memset(sc->sums, 0, sizeof(sc->sums));
+    moments_t mo;
+    memset(&mo, 0, sizeof(mo));
+    mo.pending[0] = mo.pending[1] = mo.pending[2] = -1;
     for (int i = 0; i < S; ++i) {
-        float q[3];
+        float q[3], g[3], f[3];
         point32c(entry, stepv, i, q);
         if (!finite3f(q)) status |= 2;
+        int in = inside32(q, shape);
         if (active_pose) {
-            float g[3];
-            float value = sample32(p, field, q, shape, g);
-            float y = value - mean_carry, t = mean + y;
-            mean_carry = (t - mean) - y;
-            mean = t;
+            float value = sample32c(p, field, q, shape, g, NULL);
+            blocksum_add(&mean, value, i, S);
             float alpha = ((float)i + 0.5f) * inv_s;
             for (int a = 0; a < 3; ++a) {
                 G[a] += g[a];
@@ -934,36 +1010,34 @@ static int vjp_ray_f32c(const dpt_problem* p, const void* field, const ray_t* ra
             }
         }
         if (active_volume) {
-            if (inside32(q, shape)) {
+            if (in) {
                 int lower[3];
-                float fraction[3], slope[3];
-                coordinates32(q, shape, lower, fraction, slope);
-                if (lower[0] != sc->pending[0] || lower[1] != sc->pending[1] ||
-                    lower[2] != sc->pending[2]) {
-                    if (sc->pending[0] >= 0) flush_all(sc);
-                    memset(sc->sums, 0, sizeof(sc->sums));
-                    memcpy(sc->pending, lower, sizeof(lower));
+                float slope[3];
+                coordinates32(q, shape, lower, f, slope);
+                if (lower[0] != mo.pending[0] || lower[1] != mo.pending[1] || lower[2] != mo.pending[2]) {
+                    if (mo.pending[0] >= 0) status |= flush_moments(p, &mo, volume_factor, sc->gradient);
+                    memcpy(mo.pending, lower, sizeof(lower));
                 }
-                for (int c = 0; c < 8; ++c) {
-                    float increment = scatter_increment(volume_factor, corner_weight32(fraction, c));
-                    if (bounded) {
-                        sc->sums[c] += increment;
-                    } else {
-                        if (!isfinite(increment)) status |= 2;
-                        sc->gradient[corner_index(lower, shape, c)] += (double)increment;
-                    }
-                }
-            } else if (sc->pending[0] >= 0) {
-                flush_all(sc);
-                sc->pending[0] = sc->pending[1] = sc->pending[2] = -1;
+                float fxy = f[0] * f[1];
+                mo.m[0] += 1.0f;
+                mo.m[1] += f[0];
+                mo.m[2] += f[1];
+                mo.m[3] += f[2];
+                mo.m[4] += fxy;
+                mo.m[5] += f[0] * f[2];
+                mo.m[6] += f[1] * f[2];
+                mo.m[7] += fxy * f[2];
+            } else if (mo.pending[0] >= 0) {
+                status |= flush_moments(p, &mo, volume_factor, sc->gradient);
+                mo.pending[0] = mo.pending[1] = mo.pending[2] = -1;
             }
         }
     }
-    if (active_volume && sc->pending[0] >= 0) flush_all(sc);
+    if (active_volume && mo.pending[0] >= 0) status |= flush_moments(p, &mo, volume_factor, sc->gradient);
     if (!active_pose) return status;
     const double* d = ray->r.direction;
     double Gd[3] = {G[0], G[1], G[2]}, Hd[3] = {H[0], H[1], H[2]};
-    double mean64 = (double)mean - (double)mean_carry;
+    double mean64 = (double)mean.sum - (double)mean.carry;
     double g_along = fma(Gd[2], d[2], fma(Gd[1], d[1], Gd[0] * d[0]));
     double h_along = fma(Hd[2], d[2], fma(Hd[1], d[1], Hd[0] * d[0]));
     double shift_upper = h_along, shift_lower = g_along - h_along;
