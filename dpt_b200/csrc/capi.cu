@@ -8,20 +8,26 @@ namespace dpt {
 
 int block_cols(const dpt_problem& p) { return p.block_cols == 0 ? kDefaultBlockCols : p.block_cols; }
 
-int tiles_per_view(const dpt_problem& p, int* tiles_x)
+int tile_cols(const dpt_problem& p, int threads)
+{
+    const int cols = block_cols(p);
+    return cols * 4 <= threads ? cols : threads / 4;  // at least one 8x4 warp tile per row band
+}
+
+int tiles_per_view(const dpt_problem& p, int* tiles_x, int threads)
 {
     if (p.ray_kind == DPT_RAYS_BUNDLE) {
         const int64_t rays = (int64_t)p.rows * p.cols;
-        *tiles_x = (int)((rays + kBlock - 1) / kBlock);
+        *tiles_x = (int)((rays + threads - 1) / threads);
         return *tiles_x;
     }
-    const int cols = block_cols(p), rows = kBlock / cols;
+    const int cols = tile_cols(p, threads), rows = threads / cols;
     *tiles_x = (p.cols + cols - 1) / cols;
     const int tiles_y = (p.rows + rows - 1) / rows;
     return *tiles_x * tiles_y;
 }
 
-RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status)
+RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status, int threads)
 {
     RayArgs a;
     a.grid.nx = p.nx;
@@ -35,9 +41,10 @@ RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status)
     a.cols = p.cols;
     a.samples = p.samples;
     a.ray_kind = p.ray_kind;
-    a.tiles_per_view = tiles_per_view(p, &a.tiles_x);
-    a.block_cols = block_cols(p);
-    a.block_rows = kBlock / a.block_cols;
+    a.tiles_per_view = tiles_per_view(p, &a.tiles_x, threads);
+    a.block_threads = threads;
+    a.block_cols = tile_cols(p, threads);
+    a.block_rows = threads / a.block_cols;
     a.warps_x = a.block_cols / 8;
     a.poses = r.poses;
     a.view_table = r.view_table;
@@ -99,14 +106,14 @@ int to_code(cudaError_t e) { return e == cudaSuccess ? DPT_OK : (int)e; }
 
 // Launch `body` on chunks of at most kMaxViewsPerLaunch views.
 template <typename Body>
-int chunked(const dpt_problem* p, const dpt_rays* r, int32_t* status, Body body)
+int chunked(const dpt_problem* p, const dpt_rays* r, int32_t* status, int threads, Body body)
 {
     for (int32_t first = 0; first < r->view_count; first += kMaxViewsPerLaunch) {
         dpt_rays part = *r;
         part.view_begin = r->view_begin + first;
         part.view_count = r->view_count - first < kMaxViewsPerLaunch ? r->view_count - first
                                                                       : kMaxViewsPerLaunch;
-        const dpt::RayArgs a = dpt::make_ray_args(*p, part, status);
+        const dpt::RayArgs a = dpt::make_ray_args(*p, part, status, threads);
         const int code = body(a, first);
         if (code != DPT_OK) return code;
     }
@@ -138,6 +145,8 @@ size_t dpt_b200_packed_bytes(const dpt_problem* p)
 {
     if (check_problem(p) != DPT_OK) return 0;
     if (p->layout == DPT_LAYOUT_DIRECT) return 0;
+    // compensated form: two float4 of polynomial coefficients per cell; else one 16-byte record
+    if (p->arith == DPT_ARITH_F32C) return (size_t)p->nx * p->ny * p->nz * 32u;
     return (size_t)p->nx * p->ny * p->nz * 16u;
 }
 
@@ -151,7 +160,7 @@ size_t dpt_b200_pose_partials_bytes(const dpt_problem* p, int32_t view_count)
 {
     if (check_problem(p) != DPT_OK || view_count < 1) return 0;
     int tiles_x;
-    const int tiles = dpt::tiles_per_view(*p, &tiles_x);
+    const int tiles = dpt::tiles_per_view(*p, &tiles_x, dpt::kVjpBlock);
     return (size_t)view_count * tiles * 12u * sizeof(double);
 }
 
@@ -177,7 +186,7 @@ int dpt_b200_forward(const dpt_problem* p, const dpt_rays* r, const void* packed
     if (!aligned(packed, 16)) return DPT_E_ALIGN;
     const int64_t rays_per_view = (int64_t)p->rows * p->cols;
     const size_t element = p->image_dtype == DPT_F64 ? 8 : 4;
-    return chunked(p, r, status, [&](const dpt::RayArgs& a, int32_t first) {
+    return chunked(p, r, status, dpt::kBlock, [&](const dpt::RayArgs& a, int32_t first) {
         char* out = static_cast<char*>(image) + (size_t)first * rays_per_view * element;
         return to_code(dpt::launch_forward(*p, a, packed, out, static_cast<cudaStream_t>(stream)));
     });
@@ -204,8 +213,8 @@ int dpt_b200_vjp(const dpt_problem* p, const dpt_rays* r, const void* packed,
     const int64_t rays_per_view = (int64_t)p->rows * p->cols;
     const size_t element = p->image_dtype == DPT_F64 ? 8 : 4;
     int tiles_x;
-    const int tiles = dpt::tiles_per_view(*p, &tiles_x);
-    return chunked(p, r, status, [&](const dpt::RayArgs& a, int32_t first) {
+    const int tiles = dpt::tiles_per_view(*p, &tiles_x, dpt::kVjpBlock);
+    return chunked(p, r, status, dpt::kVjpBlock, [&](const dpt::RayArgs& a, int32_t first) {
         const char* seed = static_cast<const char*>(cotangent) + (size_t)first * rays_per_view * element;
         double* partials = pose_partials;
         if (partials) {
@@ -230,7 +239,7 @@ int dpt_b200_finish_pose(const dpt_problem* p, int32_t view_begin, int32_t view_
     if (view_begin < 0 || view_count < 1 || view_begin + (int64_t)view_count > p->views)
         return DPT_E_RANGE;
     int tiles_x;
-    const int tiles = dpt::tiles_per_view(*p, &tiles_x);
+    const int tiles = dpt::tiles_per_view(*p, &tiles_x, dpt::kVjpBlock);
     return to_code(dpt::launch_finish_pose(view_begin, view_count, tiles, components, pose_partials,
                                            pose_gradient, accumulate, status,
                                            static_cast<cudaStream_t>(stream)));
@@ -258,7 +267,7 @@ int dpt_b200_counts(const dpt_problem* p, const dpt_rays* r, double* lower, doub
     if ((code = check_rays(p, r)) != DPT_OK) return code;
     if (!lower || !upper || !realised || !status) return DPT_E_NULL;
     const int64_t rays_per_view = (int64_t)p->rows * p->cols;
-    return chunked(p, r, status, [&](const dpt::RayArgs& a, int32_t first) {
+    return chunked(p, r, status, dpt::kBlock, [&](const dpt::RayArgs& a, int32_t first) {
         const int64_t offset = (int64_t)first * rays_per_view;
         return to_code(dpt::launch_counts(*p, a, lower + offset, upper + offset, realised + offset,
                                           static_cast<cudaStream_t>(stream)));

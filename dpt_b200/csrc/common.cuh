@@ -18,7 +18,15 @@
 
 namespace dpt {
 
-constexpr int kBlock = 256;      // threads per block of the ray kernels
+constexpr int kBlock = 256;      // threads per block of the forward and count kernels
+// Build-time tuning of the VJP launch (results do not depend on it beyond the FP64 order of
+// the per-block pose partials): 128-thread blocks (a 16x8 detector tile) keep five blocks of
+// the ~96-register kernel resident per SM, 20 warps against 16 with 256-thread blocks, which
+// measured 12% faster on the 256^3 / 512^2 / S=1024 full scan.
+#ifndef DPT_VJP_THREADS
+#define DPT_VJP_THREADS 128
+#endif
+constexpr int kVjpBlock = DPT_VJP_THREADS;  // threads per block of the VJP kernel
 constexpr int kDefaultBlockCols = 16;  // default block tile: 16 x 16 detector pixels
 
 struct Grid {
@@ -38,8 +46,9 @@ struct RayArgs {
     int tiles_x;         // column tiles per view (panels)
     int tiles_per_view;  // blocks per view
     int block_cols;      // detector columns per block tile (panels): 8, 16, 32 or 64
-    int block_rows;      // detector rows per block tile: 2048 / (8 * block_cols)
+    int block_rows;      // detector rows per block tile: block_threads / block_cols
     int warps_x;         // warps along the columns of a block tile: block_cols / 8
+    int block_threads;   // threads per block
     const double* poses;       // absolute view indexing
     const double* view_table;  // absolute view indexing
     const double* ray_sources;
@@ -80,7 +89,7 @@ __device__ __forceinline__ bool ray_of_thread(const RayArgs& a, int tile, int* p
 {
     const int t = threadIdx.x;
     if (a.ray_kind == DPT_RAYS_BUNDLE) {
-        const int index = tile * kBlock + t;
+        const int index = tile * a.block_threads + t;
         *pixel = index;
         return index < a.rows * a.cols;
     }
@@ -303,10 +312,21 @@ __device__ __forceinline__ void red_add_v4(float* address, float a, float b, flo
 //  Quad (FP32): quad[(z*ny+y)*nx+x] = (v(x,y,z), v(x+1,y,z), v(x,y+1,z), v(x+1,y+1,z)),
 //               indices clamped to n-1 like corner_index.  A cell reads quad at z and at
 //               min(z+1, nz-1): corners 0-3 and 4-7.
-//  Octet (FP16/BF16): all eight corners of the cell at (x,y,z) in one 16-byte record.
+//  Poly (compensated form, any storage): the cell's trilinear coefficients, two float4.
 struct QuadF32 {
+    static constexpr bool kCoefficients = false;
     const float4* quad;
     int nx, ny, nz;
+    // corners of the cell whose flat index (z*ny + y)*nx + x is `cell` (32-bit: the problem
+    // checks bound the voxel count below 2^31)
+    __device__ __forceinline__ void load_at(int cell, int, int, int lz, float* v) const
+    {
+        const float4* p = quad + cell;
+        const float4 a = __ldg(p);
+        const float4 b = __ldg(lz + 1 < nz ? p + nx * ny : p);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    }
     __device__ __forceinline__ void load(int lx, int ly, int lz, float* v) const
     {
         const int64_t plane = (int64_t)nx * ny;
@@ -320,8 +340,13 @@ struct QuadF32 {
 };
 
 struct PlainF32 {
+    static constexpr bool kCoefficients = false;
     const float* field;
     int nx, ny, nz;
+    __device__ __forceinline__ void load_at(int, int lx, int ly, int lz, float* v) const
+    {
+        load(lx, ly, lz, v);
+    }
     __device__ __forceinline__ void load(int lx, int ly, int lz, float* v) const
     {
         const int x1 = min(lx + 1, nx - 1), y1 = min(ly + 1, ny - 1), z1 = min(lz + 1, nz - 1);
@@ -334,26 +359,19 @@ struct PlainF32 {
     }
 };
 
-template <bool kBF16>
-struct OctetHalf {
-    const uint4* octet;
+// Polynomial copy (compensated precision form): per cell the FP32 coefficients c0..c7 of its
+// trilinear polynomial as two float4, formed by the pack kernel from the decoded corner values
+// with the arithmetic of PolyCache, so a sample loads its coefficients instead of its corners.
+struct PolyF32 {
+    static constexpr bool kCoefficients = true;
+    const float4* coef;
     int nx, ny, nz;
-    __device__ __forceinline__ void load(int lx, int ly, int lz, float* v) const
+    __device__ __forceinline__ void coefficients_at(int cell, float* c) const
     {
-        const uint4 r = __ldg(octet + ((int64_t)lz * ny + ly) * nx + lx);
-        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (kBF16) {
-                v[2 * k] = __uint_as_float(w[k] << 16);
-                v[2 * k + 1] = __uint_as_float(w[k] & 0xffff0000u);
-            } else {
-                const __half2 h = *reinterpret_cast<const __half2*>(&w[k]);
-                const float2 f = __half22float2(h);
-                v[2 * k] = f.x;
-                v[2 * k + 1] = f.y;
-            }
-        }
+        const float4* p = coef + 2 * (int64_t)cell;
+        const float4 a = __ldg(p), b = __ldg(p + 1);
+        c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w;
+        c[4] = b.x; c[5] = b.y; c[6] = b.z; c[7] = b.w;
     }
 };
 
@@ -466,16 +484,23 @@ __device__ __forceinline__ void inside_run(int samples, Inside inside_at, int& f
     while (last > first && !inside_at(last)) --last;
 }
 
-// Last cell's eight corner values, reloaded only when the sample enters another cell.
-template <class Field>
+// The current cell's eight corner values.  With kReuse they are reloaded only when the
+// sample enters another cell; without, every sample loads them (no branch in the loop: the
+// choice of the kernels whose loop body is long enough that the branch costs more than the
+// L1 hit it saves).
+template <class Field, bool kReuse = true>
 struct CellCache {
     float v[8];
     int cell = -1;
     __device__ __forceinline__ void fetch(const Field& f, int lx, int ly, int lz, int index)
     {
-        if (index != cell) {
-            f.load(lx, ly, lz, v);
-            cell = index;
+        if constexpr (kReuse) {
+            if (index != cell) {
+                f.load_at(index, lx, ly, lz, v);
+                cell = index;
+            }
+        } else {
+            f.load_at(index, lx, ly, lz, v);
         }
     }
 };
@@ -506,15 +531,21 @@ __device__ __forceinline__ void interior_run(int first, int last, Interior inter
 // Trilinear polynomial of a cell, f = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz,
 // formed in FP32 from the eight corner values when a ray enters the cell (the arithmetic of
 // the compensated precision form).
-template <class Field>
+template <class Field, bool kReuse = true>
 struct PolyCache {
     float c[8];
     int cell = -1;
     __device__ __forceinline__ void fetch(const Field& f, int lx, int ly, int lz, int index)
     {
-        if (index != cell) {
+        if constexpr (kReuse) {
+            if (index == cell) return;
+            cell = index;
+        }
+        if constexpr (Field::kCoefficients) {
+            f.coefficients_at(index, c);
+        } else {
             float v[8];
-            f.load(lx, ly, lz, v);
+            f.load_at(index, lx, ly, lz, v);
             c[0] = v[0];
             c[1] = v[1] - v[0];
             c[2] = v[2] - v[0];
@@ -523,7 +554,6 @@ struct PolyCache {
             c[5] = (v[5] - v[4]) - c[1];
             c[6] = (v[6] - v[4]) - c[2];
             c[7] = ((v[7] - v[6]) - (v[5] - v[4])) - c[4];
-            cell = index;
         }
     }
     // value, and when `g` is given the derivatives d/dfx, d/dfy, d/dfz

@@ -69,7 +69,7 @@ extern "C" int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_ray
                                            : (!rays->ray_sources || !rays->ray_endpoints))
         return DPT_E_NULL;
     int tiles_x;
-    const int tiles = dpt::tiles_per_view(direct, &tiles_x);
+    const int tiles = dpt::tiles_per_view(direct, &tiles_x, dpt::kVjpBlock);
     if ((size_t)rays->view_count * (size_t)tiles * (size_t)components > kPosePartialCapacity)
         return DPT_E_CAPACITY;
 
@@ -80,7 +80,7 @@ extern "C" int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_ray
     // field scan and rigid-pose check only (a null copy pointer writes no scratch)
     cudaError_t error = dpt::launch_prepare_field(direct, field, nullptr, rays->poses, status, s);
     if (error != cudaSuccess) return (int)error;
-    const dpt::RayArgs args = dpt::make_ray_args(direct, *rays, status);
+    const dpt::RayArgs args = dpt::make_ray_args(direct, *rays, status, dpt::kVjpBlock);
     error = dpt::launch_vjp(direct, args, field, cotangent,
                             components == 12 ? DPT_VJP_POSE12 : DPT_VJP_POSE6, nullptr, partials, s);
     if (error != cudaSuccess) return (int)error;

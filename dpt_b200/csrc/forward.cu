@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
     int bits = 0;
     double result = 0.0;
 
-    if (kArith == DPT_ARITH_F32) {
+    if constexpr (kArith == DPT_ARITH_F32) {
         const float o[3] = {(float)r.origin[0], (float)r.origin[1], (float)r.origin[2]};
         const float d[3] = {(float)r.direction[0], (float)r.direction[1], (float)r.direction[2]};
         const float length = (float)r.length;
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
             if (!isfinite(total)) bits |= 2;
             result = total;
         }
-    } else if (kArith == DPT_ARITH_F64) {
+    } else if constexpr (kArith == DPT_ARITH_F64) {
         if (!valid_ray(r)) {
             bits = 2;
         } else {
@@ -368,24 +368,20 @@ cudaError_t launch_forward(const dpt_problem& p, const RayArgs& a, const void* p
                            cudaStream_t stream)
 {
     const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
-    if (p.field_dtype == DPT_F32) {
-        if (p.layout == DPT_LAYOUT_DIRECT) {
-            PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
-            if (p.arith == DPT_ARITH_F32) return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
-            if (p.arith == DPT_ARITH_F64) return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
-            return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
-        }
-        QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+    if (p.arith == DPT_ARITH_F32C && p.layout == DPT_LAYOUT_REPLICATED) {
+        PolyF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+        return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
+    }
+    // FP32 storage only from here (half storage is compensated and replicated, handled above)
+    if (p.layout == DPT_LAYOUT_DIRECT) {
+        PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
         if (p.arith == DPT_ARITH_F32) return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
         if (p.arith == DPT_ARITH_F64) return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
         return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
     }
-    if (p.field_dtype == DPT_BF16) {
-        OctetHalf<true> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
-        return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
-    }
-    OctetHalf<false> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
-    return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
+    QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+    if (p.arith == DPT_ARITH_F32) return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
+    return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
 }
 
 cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower, double* upper,

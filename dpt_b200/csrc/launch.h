@@ -8,12 +8,16 @@
 
 namespace dpt {
 
-// Fill a RayArgs record for views [view_begin, view_begin + view_count).
-RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status);
+// Fill a RayArgs record for views [view_begin, view_begin + view_count) and blocks of
+// `threads` threads (kBlock for the forward and count kernels, kVjpBlock for the VJP).
+RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status, int threads);
 
 // Detector columns per block tile (panels) and blocks per view for the ray kernels.
+// Detector columns per block tile (panels), the columns a block of `threads` threads covers,
+// and blocks per view for the ray kernels.
 int block_cols(const dpt_problem& p);
-int tiles_per_view(const dpt_problem& p, int* tiles_x);
+int tile_cols(const dpt_problem& p, int threads);
+int tiles_per_view(const dpt_problem& p, int* tiles_x, int threads);
 
 cudaError_t launch_prepare_field(const dpt_problem& p, const void* field, void* packed,
                                  const double* poses, int32_t* status, cudaStream_t stream);

@@ -15,10 +15,27 @@
 // derivatives and M^T in FP64 (python/dpt/kernels/projection_fp32.py:549-602,
 // python/dpt/kernels/projection.py:1140-1217), then reduced per block with a fixed
 // warp-shuffle tree into FP64 partials that finish_pose reduces per view.
+#include <type_traits>
+
 #include "launch.h"
+
+// DPT_VJP_REUSE=1 keeps the last cell's values across samples (fewer loads, one more branch
+// per sample: 3% slower measured); DPT_VJP_MIN_BLOCKS bounds registers for that many
+// resident blocks (spills at 3 x 256 threads).
+#ifndef DPT_VJP_REUSE
+#define DPT_VJP_REUSE 0
+#endif
+#ifdef DPT_VJP_MIN_BLOCKS
+#define DPT_VJP_BOUNDS __launch_bounds__(kVjpBlock, DPT_VJP_MIN_BLOCKS)
+#else
+#define DPT_VJP_BOUNDS __launch_bounds__(kVjpBlock)
+#endif
 
 namespace dpt {
 namespace {
+
+// whether the VJP keeps the last cell's values across samples (CellCache / PolyCache kReuse)
+constexpr bool kVjpReuse = DPT_VJP_REUSE != 0;
 
 constexpr int kAlphaTable = 2048;
 
@@ -74,12 +91,12 @@ __device__ __forceinline__ void pose_epilogue(const RayArgs& a, const ViewShared
 }
 
 template <int kArith, class Field, bool kVol, bool kPose, typename Seed>
-__global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
+__global__ void DPT_VJP_BOUNDS k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
                                                 int mode, float* __restrict__ acc,
                                                 double* __restrict__ partials)
 {
     __shared__ ViewShared vs;
-    __shared__ double warp_sums[kBlock / 32][12];
+    __shared__ double warp_sums[kVjpBlock / 32][12];
     // alpha_i = (i + 0.5) / S of the FP32 pose moments, each one IEEE division, tabulated
     // once per block for the first kAlphaTable samples (later samples divide directly)
     __shared__ float alpha_table[kArith == DPT_ARITH_F32 && kPose ? kAlphaTable : 1];
@@ -87,7 +104,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
     const int view = a.view_begin + view_local;
     if (kArith == DPT_ARITH_F32 && kPose) {
         const int n = min(a.samples, kAlphaTable);
-        for (int k = threadIdx.x; k < n; k += kBlock) alpha_table[k] = ((float)k + 0.5f) / (float)a.samples;
+        for (int k = threadIdx.x; k < n; k += kVjpBlock) alpha_table[k] = ((float)k + 0.5f) / (float)a.samples;
     }
     stage_view(a, view, vs);
     int pixel;
@@ -108,7 +125,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
         FieldDims dims;
         dims.init(a.grid);
 
-        if (kArith == DPT_ARITH_F32) {
+        if constexpr (kArith == DPT_ARITH_F32) {
             const float o[3] = {(float)r.origin[0], (float)r.origin[1], (float)r.origin[2]};
             const float d[3] = {(float)r.direction[0], (float)r.direction[1], (float)r.direction[2]};
             const float length = (float)r.length;
@@ -132,12 +149,16 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
 #pragma unroll
                     for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                     int pending = -1;
-                    CellCache<Field> cache;
+                    CellCache<Field, kVjpReuse> cache;
                     auto position_at = [&](int i) { return fmaf((float)i + 0.5f, step, iv.lower); };
                     // One midpoint.  mode 0: general (support and finiteness tested); 1: on the
                     // inside run (both known to pass); 2: on the interior run (no clamp active,
                     // slope masks 1).
-                    auto visit = [&](int i, int mode) {
+                    // `bounded` (every increment finite and at most 1 in magnitude) is fixed
+                    // per ray: the march is instantiated for both values so the sample loop
+                    // carries no test of it
+                    auto visit = [&](int i, int mode, auto bounded_tag) {
+                        constexpr bool kBounded = decltype(bounded_tag)::value;
                         const bool known_inside = mode > 0;
                         const float position = position_at(i);
                         const float x = fmaf(position, d[0], o[0]);
@@ -194,7 +215,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                                     for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                                     pending = cell;
                                 }
-                                if (bounded) {
+                                if constexpr (kBounded) {
 #pragma unroll
                                     for (int c = 0; c < 8; ++c) cs[c] = cs[c] + mul_ftz(vf, w[c]);
                                 } else {
@@ -224,8 +245,9 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                             }
                         }
                     };
+                    auto march = [&](auto bounded_tag) {
                     if (!moderate(o, d)) {
-                        for (int i = 0; i < S; ++i) visit(i, 0);
+                        for (int i = 0; i < S; ++i) visit(i, 0, bounded_tag);
                     } else {
                         // samples outside the inside run add exact zeros to every moment
                         int first, last;
@@ -242,11 +264,16 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                             return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
                         }, ifirst, ilast);
                         const int split = min(ifirst, last + 1);
-                        for (int i = first; i < split; ++i) visit(i, 1);
+                        for (int i = first; i < split; ++i) visit(i, 1, bounded_tag);
 #pragma unroll 2
-                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2);
-                        for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1);
+                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2, bounded_tag);
+                        for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1, bounded_tag);
                     }
+                    };
+                    if (bounded)
+                        march(std::true_type{});
+                    else
+                        march(std::false_type{});
                     if (kVol && pending >= 0) flush_cell(acc, pending, cs);
                     if (kPose) {
                         float lo_o[3], lo_d[3], up_o[3], up_d[3];
@@ -273,7 +300,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
                     }
                 }
             }
-        } else if (kArith == DPT_ARITH_F64) {
+        } else if constexpr (kArith == DPT_ARITH_F64) {
             if (!valid_ray(r)) {
                 bits = 2;
             } else {
@@ -296,7 +323,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
 #pragma unroll
                     for (int c = 0; c < 8; ++c) cs[c] = 0.0;
                     int pending = -1;
-                    CellCache<Field> cache;
+                    CellCache<Field, kVjpReuse> cache;
                     auto flush64 = [&]() {
                         float c32[8];
 #pragma unroll
@@ -441,7 +468,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
 #pragma unroll
                     for (int c = 0; c < 8; ++c) m[c] = 0.0f;
                     int pending = -1;
-                    PolyCache<Field> cache;
+                    PolyCache<Field, kVjpReuse> cache;
                     auto flush = [&]() {
                         float corner[8];
                         corner[7] = m[7];
@@ -615,7 +642,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp(RayArgs a, Field f, const Seed* 
             if (threadIdx.x < components) {
                 double total = 0.0;
 #pragma unroll
-                for (int w = 0; w < kBlock / 32; ++w) total += warp_sums[w][threadIdx.x];
+                for (int w = 0; w < kVjpBlock / 32; ++w) total += warp_sums[w][threadIdx.x];
                 partials[((int64_t)view_local * a.tiles_per_view + blockIdx.x) * components +
                          threadIdx.x] = total;
             }
@@ -633,11 +660,11 @@ cudaError_t vjp_with(const RayArgs& a, const Field& f, const Seed* cot, int flag
     const bool pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
     const int mode = (flags & DPT_VJP_POSE12) ? 12 : ((flags & DPT_VJP_PER_RAY6) ? -6 : 6);
     if (volume && pose)
-        k_vjp<kArith, Field, true, true, Seed><<<grid, kBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+        k_vjp<kArith, Field, true, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
     else if (volume)
-        k_vjp<kArith, Field, true, false, Seed><<<grid, kBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+        k_vjp<kArith, Field, true, false, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
     else
-        k_vjp<kArith, Field, false, true, Seed><<<grid, kBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+        k_vjp<kArith, Field, false, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
     return cudaGetLastError();
 }
 
@@ -656,28 +683,23 @@ cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packe
                        const void* cotangent, int flags, float* accumulator, double* partials,
                        cudaStream_t stream)
 {
-    if (p.field_dtype == DPT_F32) {
-        if (p.layout == DPT_LAYOUT_DIRECT) {
-            PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
-            if (p.arith == DPT_ARITH_F32)
-                return vjp_seed<DPT_ARITH_F32>(p, a, f, cotangent, flags, accumulator, partials, stream);
-            if (p.arith == DPT_ARITH_F64)
-                return vjp_seed<DPT_ARITH_F64>(p, a, f, cotangent, flags, accumulator, partials, stream);
-            return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
-        }
-        QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+    if (p.arith == DPT_ARITH_F32C && p.layout == DPT_LAYOUT_REPLICATED) {
+        PolyF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+        return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
+    }
+    // FP32 storage only from here (half storage is compensated and replicated, handled above)
+    if (p.layout == DPT_LAYOUT_DIRECT) {
+        PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
         if (p.arith == DPT_ARITH_F32)
             return vjp_seed<DPT_ARITH_F32>(p, a, f, cotangent, flags, accumulator, partials, stream);
         if (p.arith == DPT_ARITH_F64)
             return vjp_seed<DPT_ARITH_F64>(p, a, f, cotangent, flags, accumulator, partials, stream);
         return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
     }
-    if (p.field_dtype == DPT_BF16) {
-        OctetHalf<true> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
-        return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
-    }
-    OctetHalf<false> f{static_cast<const uint4*>(packed), p.nx, p.ny, p.nz};
-    return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
+    QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+    if (p.arith == DPT_ARITH_F32)
+        return vjp_seed<DPT_ARITH_F32>(p, a, f, cotangent, flags, accumulator, partials, stream);
+    return vjp_seed<DPT_ARITH_F64>(p, a, f, cotangent, flags, accumulator, partials, stream);
 }
 
 }  // namespace dpt
