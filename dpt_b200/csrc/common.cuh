@@ -571,6 +571,153 @@ struct PolyCache {
     }
 };
 
+// ------------------------------------------------ compensated form: cell runs in closed form
+//
+// For rays whose grid origin and direction stay below 1e30, the samples inside the support,
+// [first, last], are grouped into runs of consecutive samples in one interpolation cell by
+// walking the cell planes along the ray.  Along a run the fractions are f + j d (j = 0..n-1,
+// d the per-sample step; d = 0 on an axis in its half-cell margin, whose fraction is clamped),
+// so the run's sum of the cell polynomial, its slope sums and the volume moments are
+// polynomials in j of degree <= 3: closed forms in the power sums S1 = sum j, S2 = sum j^2,
+// S3 = sum j^3.  Cost per cell crossed instead of per sample.
+
+struct CellRun {
+    int i0, n;             // first sample of the run and its sample count
+    int lx, ly, lz, cell;  // interpolation cell (lower corner, clamped) and its flat index
+    int interior;          // bit k set: axis k inside its cell range (its slope is active)
+    float f[3], d[3];      // fractions at sample i0 and their change per sample
+    float nf, s1, s2, s3;  // n and the power sums of j over 0..n-1
+};
+
+__device__ __forceinline__ float plane_crossing(const float* entry, const float* inverse,
+                                                const float* sv, const int* axis_cell,
+                                                const int* shape, int k)
+{
+    if (sv[k] > 0.0f && axis_cell[k] + 1 <= shape[k] - 1)
+        return ((float)(axis_cell[k] + 1) - entry[k]) * inverse[k];
+    if (sv[k] < 0.0f && axis_cell[k] >= 0) return ((float)axis_cell[k] - entry[k]) * inverse[k];
+    return __int_as_float(0x7f800000);  // +inf: no plane left inside the support
+}
+
+// Walk the cell planes from sample `first` to `last` (sample i at entry + (i + 0.5) sv) and
+// call `action(run)` for every run with at least one sample.  Each step advances every axis
+// whose plane is the nearest, so the walk ends within nx + ny + nz + 3 steps.
+template <typename Action>
+__device__ __forceinline__ void walk_cells(const FieldDims& dims, const float* entry, const float* sv,
+                                           int first, int last, Action action)
+{
+    const int shape[3] = {dims.nx, dims.ny, dims.nz};
+    float inverse[3], next[3];
+    int axis_cell[3];
+    {
+        const float offset = (float)first + 0.5f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int c = (int)floorf(fmaf(offset, sv[k], entry[k]));
+            axis_cell[k] = c < -1 ? -1 : (c > shape[k] - 1 ? shape[k] - 1 : c);
+            inverse[k] = sv[k] != 0.0f ? 1.0f / sv[k] : 0.0f;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) next[k] = plane_crossing(entry, inverse, sv, axis_cell, shape, k);
+    int i = first;
+    const int limit = shape[0] + shape[1] + shape[2] + 4;
+    for (int walk = 0; walk < limit; ++walk) {
+        const float nearest = fminf(next[0], fminf(next[1], next[2]));
+        const float t = nearest - 0.5f;
+        const int end = !(t < (float)(last + 1)) ? last + 1 : (t <= (float)i ? i : (int)ceilf(t));
+        if (end > i) {
+            CellRun r;
+            r.i0 = i;
+            r.n = end - i;
+            const float offset = (float)i + 0.5f;
+            int lower[3];
+            r.interior = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int top = shape[k] - 2 < 0 ? 0 : shape[k] - 2;
+                if (axis_cell[k] >= 0 && axis_cell[k] <= shape[k] - 2) {
+                    lower[k] = axis_cell[k];
+                    r.f[k] = fmaf(offset, sv[k], entry[k]) - (float)axis_cell[k];
+                    r.d[k] = sv[k];
+                    r.interior |= 1 << k;
+                } else {
+                    lower[k] = axis_cell[k] < 0 ? 0 : top;
+                    r.f[k] = (axis_cell[k] < 0 || shape[k] == 1) ? 0.0f : 1.0f;
+                    r.d[k] = 0.0f;
+                }
+            }
+            r.lx = lower[0];
+            r.ly = lower[1];
+            r.lz = lower[2];
+            r.cell = (lower[2] * dims.ny + lower[1]) * dims.nx + lower[0];
+            const int64_t m = r.n;
+            r.nf = (float)m;
+            r.s1 = (float)(m * (m - 1) / 2);
+            r.s2 = (float)(m * (m - 1) * (2 * m - 1) / 6);
+            r.s3 = r.s1 * r.s1;
+            action(r);
+        }
+        i = end;
+        if (i > last) break;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (next[k] == nearest) {
+                axis_cell[k] += sv[k] > 0.0f ? 1 : -1;
+                next[k] = plane_crossing(entry, inverse, sv, axis_cell, shape, k);
+            }
+        }
+    }
+}
+
+// The run cell's polynomial at the run's first fractions: value, slopes d/dfx, d/dfy, d/dfz and
+// the bilinear terms a = c4 + c7 z, t1 = c5 + c7 y, t2 = c6 + c7 x (the arithmetic of
+// PolyCache::eval, extended).
+struct RunPoly {
+    float value, gx, gy, gz, a, t1, t2, c7;
+};
+
+__device__ __forceinline__ RunPoly run_poly(const float* c, const float* f)
+{
+    RunPoly o;
+    const float fx = f[0], fy = f[1], fz = f[2];
+    o.a = fmaf(c[7], fz, c[4]);
+    const float b = fmaf(c[5], fz, c[1]);
+    o.gx = fmaf(o.a, fy, b);
+    const float e = fmaf(c[6], fz, c[2]), h = fmaf(c[3], fz, c[0]);
+    o.value = fmaf(o.gx, fx, fmaf(e, fy, h));
+    o.gy = fmaf(o.a, fx, e);
+    o.t1 = fmaf(c[7], fy, c[5]);
+    o.t2 = fmaf(c[7], fx, c[6]);
+    o.gz = fmaf(fx, o.t1, fmaf(c[6], fy, c[3]));
+    o.c7 = c[7];
+    return o;
+}
+
+// Sum over the run of the cell polynomial: n A + S1 B + S2 C + S3 D.
+__device__ __forceinline__ float run_sum(const CellRun& r, const RunPoly& o)
+{
+    const float dx = r.d[0], dy = r.d[1], dz = r.d[2];
+    const float dxy = dx * dy, dxz = dx * dz, dyz = dy * dz;
+    const float B = fmaf(o.gz, dz, fmaf(o.gy, dy, o.gx * dx));
+    const float C = fmaf(o.t2, dyz, fmaf(o.t1, dxz, o.a * dxy));
+    const float D = o.c7 * (dxy * dz);
+    return fmaf(r.s3, D, fmaf(r.s2, C, fmaf(r.s1, B, r.nf * o.value)));
+}
+
+// Kahan-compensated FP32 sum.
+struct Kahan32 {
+    float sum = 0.0f, carry = 0.0f;
+    __device__ __forceinline__ void add(float value)
+    {
+        const float y = value - carry;
+        const float t = sum + y;
+        carry = (t - sum) - y;
+        sum = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)sum - (double)carry; }
+};
+
 // Compensated ray sum of the precision form: 16-sample blocks summed serially in FP32,
 // block sums added with Kahan compensation.  Blocks are aligned to the sample index.
 struct BlockSum {

@@ -10,9 +10,10 @@
 //          midpoints, fmaf corner sum, serial FP32 total, total *= length*step)
 //   F64  - python/dpt/kernels/projection.py:802-846 with the midpoint integrator 770-799
 //   F32C - FP64 setup and clip; FP32 marching p_i = entry + (i+0.5) step_vector (the mixed
-//          recurrence of python/dpt/kernels/projection.py:368-392), FP32 samples from the
-//          cell's trilinear polynomial and a blocked compensated FP32 ray sum scaled by
-//          length*step in FP64 (the precision form of this build, no reference counterpart).
+//          recurrence of python/dpt/kernels/projection.py:368-392); the samples of each cell
+//          run summed in closed form from the cell's trilinear polynomial, the run sums added
+//          with Kahan compensation and scaled by length*step in FP64 (the precision form of
+//          this build, no reference counterpart).
 //
 // Samples inside the support form one run; within it the interior run (0 <= p < n-1 on every
 // axis) skips the clamps of the cell coordinate.  Both are exact rewrites of the per-sample
@@ -213,60 +214,52 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                     entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
                     sv[k] = (float)(step * r.direction[k]);
                 }
-                BlockSum acc;
                 auto at = [&](int i, float& x, float& y, float& z) {
                     const float offset = (float)i + 0.5f;
                     x = fmaf(offset, sv[0], entry[0]);
                     y = fmaf(offset, sv[1], entry[1]);
                     z = fmaf(offset, sv[2], entry[2]);
                 };
-                PolyCache<Field> cache;
-                auto add = [&](int i, Axis32 X, Axis32 Y, Axis32 Z) {
-                    cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
-                    acc.add(cache.eval(X.fraction, Y.fraction, Z.fraction), i, S);
-                };
-                auto margin = [&](int i) {
-                    float x, y, z;
-                    at(i, x, y, z);
-                    if (inside(x, y, z, dims.hx, dims.hy, dims.hz))
-                        add(i, axis32(x, dims.mx, dims.cx), axis32(y, dims.my, dims.cy), axis32(z, dims.mz, dims.cz));
-                    else
-                        acc.add(0.0f, i, S);
-                };
+                double total;
                 if (!moderate(entry, sv)) {
+                    // per-sample form: polynomial samples, blocked compensated sum
+                    BlockSum acc;
+                    PolyCache<Field> cache;
                     bool finite = true;
                     for (int i = 0; i < S; ++i) {
                         float x, y, z;
                         at(i, x, y, z);
                         finite = finite && finite3f(x, y, z);
-                        margin(i);
+                        if (inside(x, y, z, dims.hx, dims.hy, dims.hz)) {
+                            const Axis32 X = axis32(x, dims.mx, dims.cx), Y = axis32(y, dims.my, dims.cy),
+                                         Z = axis32(z, dims.mz, dims.cz);
+                            cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
+                            acc.add(cache.eval(X.fraction, Y.fraction, Z.fraction), i, S);
+                        } else {
+                            acc.add(0.0f, i, S);
+                        }
                     }
                     if (!finite) bits |= 2;
+                    total = acc.value();
                 } else {
+                    // segment form: closed-form sums over the cell runs, compensated across runs
                     int first, last;
                     inside_run(S, [&](int i) {
                         float x, y, z;
                         at(i, x, y, z);
                         return inside(x, y, z, dims.hx, dims.hy, dims.hz);
                     }, first, last);
-                    int ifirst, ilast;
-                    interior_run(first, last, [&](int i) {
-                        float x, y, z;
-                        at(i, x, y, z);
-                        return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
-                    }, ifirst, ilast);
-                    const int split = min(ifirst, last + 1);
-                    for (int i = first; i < split; ++i) margin(i);
-#pragma unroll 4
-                    for (int i = ifirst; i <= ilast; ++i) {
-                        float x, y, z;
-                        at(i, x, y, z);
-                        add(i, interior_axis(x), interior_axis(y), interior_axis(z));
+                    Kahan32 acc;
+                    if (first <= last) {
+                        walk_cells(dims, entry, sv, first, last, [&](const CellRun& run) {
+                            PolyCache<Field, false> cell;
+                            cell.fetch(f, run.lx, run.ly, run.lz, run.cell);
+                            acc.add(run_sum(run, run_poly(cell.c, run.f)));
+                        });
                     }
-                    for (int i = max(ilast + 1, split); i <= last; ++i) margin(i);
-                    acc.finish(max(last, first - 1), S);
+                    total = acc.value();
                 }
-                result = acc.value() * (r.length * step);
+                result = total * (r.length * step);
             }
             if (!finite_out<Out>(result)) bits |= 2;
         }

@@ -440,10 +440,10 @@ __global__ void DPT_VJP_BOUNDS k_vjp(RayArgs a, Field f, const Seed* __restrict_
                 }
             }
         } else {
-            // F32C: FP64 clip; FP32 marching; value and slope from the cell's trilinear
-            // polynomial; blocked compensated mean; pose moments G = sum grad, H = sum alpha
-            // grad; volume scatter through per-run moments of the fractions, expanded into
-            // the eight corner sums at the end of each cell run.
+            // F32C: FP64 clip; FP32 marching; per cell run (closed form over the run's
+            // samples): the compensated mean, pose sums G = sum grad and H = sum alpha grad
+            // from the cell's trilinear polynomial, and the eight moments of the fractions
+            // expanded into the cell's eight corner sums.
             if (!valid_ray(r)) {
                 bits = 2;
             } else {
@@ -461,15 +461,9 @@ __global__ void DPT_VJP_BOUNDS k_vjp(RayArgs a, Field f, const Seed* __restrict_
                         entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
                         sv[k] = (float)(step * r.direction[k]);
                     }
-                    const float inv_s = 1.0f / (float)S;
-                    BlockSum mean;
-                    float G[3] = {0.0f, 0.0f, 0.0f}, H[3] = {0.0f, 0.0f, 0.0f};
-                    float m[8];
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) m[c] = 0.0f;
-                    int pending = -1;
-                    PolyCache<Field, kVjpReuse> cache;
-                    auto flush = [&]() {
+                    double mean64 = 0.0, Gd[3] = {0.0, 0.0, 0.0}, Hd[3] = {0.0, 0.0, 0.0};
+                    // eight moments of a run's fractions -> its cell's eight corner sums, scaled
+                    auto scatter_moments = [&](int cell, const float* m) {
                         float corner[8];
                         corner[7] = m[7];
                         corner[3] = m[4] - m[7];
@@ -484,106 +478,153 @@ __global__ void DPT_VJP_BOUNDS k_vjp(RayArgs a, Field f, const Seed* __restrict_
                         for (int c = 0; c < 8; ++c) {
                             corner[c] = vf * corner[c];
                             finite = finite && isfinite(corner[c]);
-                            m[c] = 0.0f;
                         }
                         if (!finite) bits |= 2;
-                        flush_cell(acc, pending, corner);
+                        flush_cell(acc, cell, corner);
                     };
-                    auto point_at = [&](int i, float& x, float& y, float& z) {
-                        const float offset = (float)i + 0.5f;
-                        x = fmaf(offset, sv[0], entry[0]);
-                        y = fmaf(offset, sv[1], entry[1]);
-                        z = fmaf(offset, sv[2], entry[2]);
-                    };
-                    // mode 0: general; 1: inside run; 2: interior run
-                    auto visit = [&](int i, int mode) {
-                        float x, y, z;
-                        point_at(i, x, y, z);
-                        bool in = true;
-                        if (mode == 0) {
-                            if (!finite3f(x, y, z)) bits |= 2;
-                            in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                    if (moderate(entry, sv)) {
+                        // segment form: every cell run in closed form
+                        int first, last;
+                        inside_run(S, [&](int i) {
+                            const float offset = (float)i + 0.5f;
+                            return inside(fmaf(offset, sv[0], entry[0]), fmaf(offset, sv[1], entry[1]),
+                                          fmaf(offset, sv[2], entry[2]), dims.hx, dims.hy, dims.hz);
+                        }, first, last);
+                        Kahan32 mean;
+                        float G[3] = {0.0f, 0.0f, 0.0f}, Hs[3] = {0.0f, 0.0f, 0.0f};
+                        if (first <= last) {
+                            walk_cells(dims, entry, sv, first, last, [&](const CellRun& run) {
+                                const float dx = run.d[0], dy = run.d[1], dz = run.d[2];
+                                const float dxy = dx * dy, dxz = dx * dz, dyz = dy * dz;
+                                const float nf = run.nf, s1 = run.s1, s2 = run.s2, s3 = run.s3;
+                                if (kPose) {
+                                    PolyCache<Field, false> cell;
+                                    cell.fetch(f, run.lx, run.ly, run.lz, run.cell);
+                                    const RunPoly o = run_poly(cell.c, run.f);
+                                    mean.add(run_sum(run, o));
+                                    float g0[3] = {o.gx, o.gy, o.gz};
+                                    float g1[3] = {fmaf(o.t1, dz, o.a * dy), fmaf(o.t2, dz, o.a * dx),
+                                                   fmaf(o.t2, dy, o.t1 * dx)};
+                                    float g2[3] = {o.c7 * dyz, o.c7 * dxz, o.c7 * dxy};
+                                    const float offset = (float)run.i0 + 0.5f;
+#pragma unroll
+                                    for (int k = 0; k < 3; ++k) {
+                                        if (!((run.interior >> k) & 1)) g0[k] = g1[k] = g2[k] = 0.0f;
+                                        const float sg = fmaf(s2, g2[k], fmaf(s1, g1[k], nf * g0[k]));
+                                        const float sj = fmaf(s3, g2[k], fmaf(s2, g1[k], s1 * g0[k]));
+                                        G[k] = G[k] + sg;
+                                        Hs[k] = Hs[k] + fmaf(offset, sg, sj);
+                                    }
+                                }
+                                if (kVol) {
+                                    const float fx = run.f[0], fy = run.f[1], fz = run.f[2];
+                                    const float fxy = fx * fy, fxz = fx * fz, fyz = fy * fz;
+                                    float m[8];
+                                    m[0] = nf;
+                                    m[1] = fmaf(s1, dx, nf * fx);
+                                    m[2] = fmaf(s1, dy, nf * fy);
+                                    m[3] = fmaf(s1, dz, nf * fz);
+                                    m[4] = fmaf(s2, dxy, fmaf(s1, fmaf(fx, dy, fy * dx), nf * fxy));
+                                    m[5] = fmaf(s2, dxz, fmaf(s1, fmaf(fx, dz, fz * dx), nf * fxz));
+                                    m[6] = fmaf(s2, dyz, fmaf(s1, fmaf(fy, dz, fz * dy), nf * fyz));
+                                    m[7] = fmaf(s3, dxy * dz,
+                                                fmaf(s2, fmaf(fz, dxy, fmaf(fy, dxz, fx * dyz)),
+                                                     fmaf(s1, fmaf(fyz, dx, fmaf(fxz, dy, fxy * dz)),
+                                                          nf * (fxy * fz))));
+                                    scatter_moments(run.cell, m);
+                                }
+                            });
                         }
-                        Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
-                        int cell = -1;
-                        if (mode == 2) {
-                            X = interior_axis(x);
-                            Y = interior_axis(y);
-                            Z = interior_axis(z);
-                        } else if (in) {
-                            X = axis32(x, dims.mx, dims.cx);
-                            Y = axis32(y, dims.my, dims.cy);
-                            Z = axis32(z, dims.mz, dims.cz);
-                        }
-                        if (in) cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
                         if (kPose) {
-                            float value = 0.0f, gs[3] = {0.0f, 0.0f, 0.0f};
+                            mean64 = mean.value();
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                Gd[k] = G[k];
+                                Hd[k] = (double)Hs[k] / (double)S;
+                            }
+                        }
+                    } else {
+                        // per-sample form (rays reaching 1e30 in grid coordinates)
+                        const float inv_s = 1.0f / (float)S;
+                        BlockSum mean;
+                        float G[3] = {0.0f, 0.0f, 0.0f}, H[3] = {0.0f, 0.0f, 0.0f};
+                        float m[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) m[c] = 0.0f;
+                        int pending = -1;
+                        PolyCache<Field, kVjpReuse> cache;
+                        for (int i = 0; i < S; ++i) {
+                            const float offset = (float)i + 0.5f;
+                            const float x = fmaf(offset, sv[0], entry[0]);
+                            const float y = fmaf(offset, sv[1], entry[1]);
+                            const float z = fmaf(offset, sv[2], entry[2]);
+                            if (!finite3f(x, y, z)) bits |= 2;
+                            const bool in = inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                            Axis32 X{0, 0.0f}, Y{0, 0.0f}, Z{0, 0.0f};
+                            int cell = -1;
                             if (in) {
-                                cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
-                                value = cache.eval(X.fraction, Y.fraction, Z.fraction, gs);
-                                if (mode != 2) {
+                                X = axis32(x, dims.mx, dims.cx);
+                                Y = axis32(y, dims.my, dims.cy);
+                                Z = axis32(z, dims.mz, dims.cz);
+                                cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
+                            }
+                            if (kPose) {
+                                float value = 0.0f, gs[3] = {0.0f, 0.0f, 0.0f};
+                                if (in) {
+                                    cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
+                                    value = cache.eval(X.fraction, Y.fraction, Z.fraction, gs);
                                     if (!(x >= 0.0f && x < dims.mx)) gs[0] = 0.0f * gs[0];
                                     if (!(y >= 0.0f && y < dims.my)) gs[1] = 0.0f * gs[1];
                                     if (!(z >= 0.0f && z < dims.mz)) gs[2] = 0.0f * gs[2];
                                 }
+                                mean.add(value, i, S);
+                                const float alpha = offset * inv_s;
+#pragma unroll
+                                for (int k = 0; k < 3; ++k) {
+                                    G[k] = G[k] + gs[k];
+                                    H[k] = fmaf(alpha, gs[k], H[k]);
+                                }
                             }
-                            mean.add(value, i, S);
-                            const float alpha = ((float)i + 0.5f) * inv_s;
+                            if (kVol) {
+                                if (in) {
+                                    if (cell != pending) {
+                                        if (pending >= 0) {
+                                            scatter_moments(pending, m);
+#pragma unroll
+                                            for (int c = 0; c < 8; ++c) m[c] = 0.0f;
+                                        }
+                                        pending = cell;
+                                    }
+                                    const float fx = X.fraction, fy = Y.fraction, fz = Z.fraction;
+                                    const float fxy = fx * fy;
+                                    m[0] = m[0] + 1.0f;
+                                    m[1] = m[1] + fx;
+                                    m[2] = m[2] + fy;
+                                    m[3] = m[3] + fz;
+                                    m[4] = m[4] + fxy;
+                                    m[5] = m[5] + fx * fz;
+                                    m[6] = m[6] + fy * fz;
+                                    m[7] = m[7] + fxy * fz;
+                                } else if (pending >= 0) {
+                                    scatter_moments(pending, m);
+#pragma unroll
+                                    for (int c = 0; c < 8; ++c) m[c] = 0.0f;
+                                    pending = -1;
+                                }
+                            }
+                        }
+                        if (kVol && pending >= 0) scatter_moments(pending, m);
+                        if (kPose) {
+                            mean64 = mean.value();
 #pragma unroll
                             for (int k = 0; k < 3; ++k) {
-                                G[k] = G[k] + gs[k];
-                                H[k] = fmaf(alpha, gs[k], H[k]);
+                                Gd[k] = G[k];
+                                Hd[k] = H[k];
                             }
                         }
-                        if (kVol) {
-                            if (in) {
-                                if (cell != pending) {
-                                    if (pending >= 0) flush();
-                                    pending = cell;
-                                }
-                                const float fx = X.fraction, fy = Y.fraction, fz = Z.fraction;
-                                const float fxy = fx * fy;
-                                m[0] = m[0] + 1.0f;
-                                m[1] = m[1] + fx;
-                                m[2] = m[2] + fy;
-                                m[3] = m[3] + fz;
-                                m[4] = m[4] + fxy;
-                                m[5] = m[5] + fx * fz;
-                                m[6] = m[6] + fy * fz;
-                                m[7] = m[7] + fxy * fz;
-                            } else if (pending >= 0) {
-                                flush();
-                                pending = -1;
-                            }
-                        }
-                    };
-                    if (!moderate(entry, sv)) {
-                        for (int i = 0; i < S; ++i) visit(i, 0);
-                    } else {
-                        int first, last;
-                        inside_run(S, [&](int i) {
-                            float x, y, z;
-                            point_at(i, x, y, z);
-                            return inside(x, y, z, dims.hx, dims.hy, dims.hz);
-                        }, first, last);
-                        int ifirst, ilast;
-                        interior_run(first, last, [&](int i) {
-                            float x, y, z;
-                            point_at(i, x, y, z);
-                            return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
-                        }, ifirst, ilast);
-                        const int split = min(ifirst, last + 1);
-                        for (int i = first; i < split; ++i) visit(i, 1);
-#pragma unroll 2
-                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2);
-                        for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1);
-                        if (kPose) mean.finish(max(last, first - 1), S);
                     }
-                    if (kVol && pending >= 0) flush();
                     if (kPose) {
                         const double* dr = r.direction;
-                        const double Gd[3] = {G[0], G[1], G[2]}, Hd[3] = {H[0], H[1], H[2]};
-                        const double mean64 = mean.value();
                         const double g_along = fma(Gd[2], dr[2], fma(Gd[1], dr[1], Gd[0] * dr[0]));
                         const double h_along = fma(Hd[2], dr[2], fma(Hd[1], dr[1], Hd[0] * dr[0]));
                         const double su = h_along, sl = g_along - h_along;

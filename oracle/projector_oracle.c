@@ -502,6 +502,202 @@ static void point32c(const float* entry, const float* step_vector, int index, fl
         q[a] = fmaf(offset, step_vector[a], entry[a]);
 }
 
+/* ------------------------------------------------- F32C segment form (moderate rays)
+ * The samples inside the support, [first, last], are grouped into runs of consecutive
+ * samples in one interpolation cell by walking the cell planes along the ray.  Along the
+ * run the fractions are f + j d (j = 0..n-1, d the per-sample step; d = 0 on an axis in its
+ * half-cell margin, where the fraction is clamped), so the run's sum of the cell polynomial,
+ * its slope sums and the volume moments are polynomials in j of degree <= 3, evaluated in
+ * closed form with the power sums S1 = sum j, S2 = sum j^2, S3 = sum j^3.  Rays whose grid
+ * origin or direction reach 1e30 take the per-sample form instead. */
+
+static int moderate32c(const float* entry, const float* step_vector)
+{
+    float m = 0.0f;
+    for (int a = 0; a < 3; ++a) {
+        m = fmaxf(m, fabsf(entry[a]));
+        m = fmaxf(m, fabsf(step_vector[a]));
+    }
+    return m < 1e30f;
+}
+
+/* First and last samples inside the support (first > last when none): the points are
+ * monotone in the sample index on every axis, so the inside samples form one run. */
+static void inside_run32c(const float* entry, const float* step_vector, const int* shape, int S,
+                          int* first, int* last)
+{
+    float q[3];
+    int f = 0, l = S - 1;
+    for (; f <= l; ++f) {
+        point32c(entry, step_vector, f, q);
+        if (inside32(q, shape)) break;
+    }
+    for (; l > f; --l) {
+        point32c(entry, step_vector, l, q);
+        if (inside32(q, shape)) break;
+    }
+    *first = f;
+    *last = l;
+}
+
+typedef struct {
+    int i0, n;        /* first sample of the run and its sample count */
+    int cell[3];      /* interpolation cell (lower corner, clamped to the grid) */
+    int interior[3];  /* 1 where the axis lies inside its cell range (slope active) */
+    float f[3], d[3]; /* fractions at sample i0 and their per-sample change */
+    float nf, s1, s2, s3;
+} run32c_t;
+
+/* sample-index coordinate u (sample i at u = i + 0.5) where the ray meets the next cell
+ * plane on axis k, or +inf when none is left inside the support */
+static float crossing32c(const float* entry, const float* inverse, const float* step_vector,
+                         const int* plane_cell, const int* shape, int k)
+{
+    if (step_vector[k] > 0.0f && plane_cell[k] + 1 <= shape[k] - 1)
+        return ((float)(plane_cell[k] + 1) - entry[k]) * inverse[k];
+    if (step_vector[k] < 0.0f && plane_cell[k] >= 0)
+        return ((float)plane_cell[k] - entry[k]) * inverse[k];
+    return INFINITY;
+}
+
+static void make_run32c(const float* entry, const float* step_vector, const int* shape,
+                        const int* axis_cell, int i0, int n, run32c_t* r)
+{
+    float q[3];
+    point32c(entry, step_vector, i0, q);
+    r->i0 = i0;
+    r->n = n;
+    for (int k = 0; k < 3; ++k) {
+        const int top = shape[k] - 2 < 0 ? 0 : shape[k] - 2;
+        if (axis_cell[k] >= 0 && axis_cell[k] <= shape[k] - 2) {
+            r->cell[k] = axis_cell[k];
+            r->f[k] = q[k] - (float)axis_cell[k];
+            r->d[k] = step_vector[k];
+            r->interior[k] = 1;
+        } else {
+            r->cell[k] = axis_cell[k] < 0 ? 0 : top;
+            r->f[k] = (axis_cell[k] < 0 || shape[k] == 1) ? 0.0f : 1.0f;
+            r->d[k] = 0.0f;
+            r->interior[k] = 0;
+        }
+    }
+    const int64_t m = n;
+    r->nf = (float)m;
+    r->s1 = (float)(m * (m - 1) / 2);
+    r->s2 = (float)(m * (m - 1) * (2 * m - 1) / 6);
+    r->s3 = r->s1 * r->s1;
+}
+
+typedef void (*run_action32c)(void* context, const run32c_t* run);
+
+/* Walk the cell planes from sample `first` to `last`, calling `action` on every run with at
+ * least one sample.  Each step advances every axis whose plane is the nearest, so the walk
+ * ends after at most nx + ny + nz + 3 steps. */
+static void traverse32c(const float* entry, const float* step_vector, const int* shape, int first,
+                        int last, run_action32c action, void* context)
+{
+    float q[3], inverse[3], next[3];
+    int axis_cell[3];
+    point32c(entry, step_vector, first, q);
+    for (int k = 0; k < 3; ++k) {
+        int c = (int)floorf(q[k]);
+        axis_cell[k] = c < -1 ? -1 : (c > shape[k] - 1 ? shape[k] - 1 : c);
+        inverse[k] = step_vector[k] != 0.0f ? 1.0f / step_vector[k] : 0.0f;
+    }
+    for (int k = 0; k < 3; ++k) next[k] = crossing32c(entry, inverse, step_vector, axis_cell, shape, k);
+    int i = first;
+    const int limit = shape[0] + shape[1] + shape[2] + 4;
+    for (int walk = 0; walk < limit; ++walk) {
+        const float nearest = fminf(next[0], fminf(next[1], next[2]));
+        const float t = nearest - 0.5f;
+        const int end = !(t < (float)(last + 1)) ? last + 1 : (t <= (float)i ? i : (int)ceilf(t));
+        if (end > i) {
+            run32c_t run;
+            make_run32c(entry, step_vector, shape, axis_cell, i, end - i, &run);
+            action(context, &run);
+        }
+        i = end;
+        if (i > last) break;
+        for (int k = 0; k < 3; ++k) {
+            if (next[k] == nearest) {
+                axis_cell[k] += step_vector[k] > 0.0f ? 1 : -1;
+                next[k] = crossing32c(entry, inverse, step_vector, axis_cell, shape, k);
+            }
+        }
+    }
+}
+
+/* The cell polynomial f = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz of the run's
+ * cell and its value and slopes at the run's first fractions. */
+typedef struct {
+    float c[8];
+    float value, gx, gy, gz;
+    float a, t1, t2; /* c4 + c7 z, c5 + c7 y, c6 + c7 x */
+} runpoly32c_t;
+
+static void run_poly32c(const dpt_problem* p, const void* field, const run32c_t* r, runpoly32c_t* o)
+{
+    int shape[3] = {p->nx, p->ny, p->nz};
+    float v[8];
+    for (int c = 0; c < 8; ++c) v[c] = field_value(p, field, corner_index(r->cell, shape, c));
+    float* c = o->c;
+    c[0] = v[0];
+    c[1] = v[1] - v[0];
+    c[2] = v[2] - v[0];
+    c[3] = v[4] - v[0];
+    c[4] = (v[3] - v[2]) - c[1];
+    c[5] = (v[5] - v[4]) - c[1];
+    c[6] = (v[6] - v[4]) - c[2];
+    c[7] = ((v[7] - v[6]) - (v[5] - v[4])) - c[4];
+    const float fx = r->f[0], fy = r->f[1], fz = r->f[2];
+    o->a = fmaf(c[7], fz, c[4]);
+    const float b = fmaf(c[5], fz, c[1]);
+    o->gx = fmaf(o->a, fy, b);
+    const float e = fmaf(c[6], fz, c[2]), h = fmaf(c[3], fz, c[0]);
+    o->value = fmaf(o->gx, fx, fmaf(e, fy, h));
+    o->gy = fmaf(o->a, fx, e);
+    o->t1 = fmaf(c[7], fy, c[5]);
+    o->t2 = fmaf(c[7], fx, c[6]);
+    o->gz = fmaf(fx, o->t1, fmaf(c[6], fy, c[3]));
+}
+
+/* sum over the run of the cell polynomial: n A + S1 B + S2 C + S3 D */
+static float run_sum32c(const run32c_t* r, const runpoly32c_t* o)
+{
+    const float dx = r->d[0], dy = r->d[1], dz = r->d[2];
+    const float dxy = dx * dy, dxz = dx * dz, dyz = dy * dz;
+    const float B = fmaf(o->gz, dz, fmaf(o->gy, dy, o->gx * dx));
+    const float C = fmaf(o->t2, dyz, fmaf(o->t1, dxz, o->a * dxy));
+    const float D = o->c[7] * (dxy * dz);
+    return fmaf(r->s3, D, fmaf(r->s2, C, fmaf(r->s1, B, r->nf * o->value)));
+}
+
+typedef struct {
+    float sum, carry;
+} kahan32_t;
+
+static void kahan_add32(kahan32_t* k, float value)
+{
+    const float y = value - k->carry;
+    const float t = k->sum + y;
+    k->carry = (t - k->sum) - y;
+    k->sum = t;
+}
+
+typedef struct {
+    const dpt_problem* p;
+    const void* field;
+    kahan32_t total;
+} fwd_context32c;
+
+static void forward_action32c(void* context, const run32c_t* run)
+{
+    fwd_context32c* ctx = (fwd_context32c*)context;
+    runpoly32c_t o;
+    run_poly32c(ctx->p, ctx->field, run, &o);
+    kahan_add32(&ctx->total, run_sum32c(run, &o));
+}
+
 /* ------------------------------------------------------------------ forward */
 
 /* One ray's optical depth; returns status bits. */
@@ -548,16 +744,26 @@ static int forward_ray(const dpt_problem* p, const void* field, const ray_t* ray
         double integral = 0.0;
         if (iv->upper > iv->lower) {
             float entry[3], stepv[3];
-            blocksum_t acc = {0.0f, 0.0f, 0.0f};
             march32c(ray, S, entry, stepv);
-            for (int i = 0; i < S; ++i) {
-                float q[3];
-                point32c(entry, stepv, i, q);
-                if (!finite3f(q)) status |= 2;
-                blocksum_add(&acc, sample32c(p, field, q, shape, NULL, NULL), i, S);
+            double total;
+            if (moderate32c(entry, stepv)) {
+                int first, last;
+                inside_run32c(entry, stepv, shape, S, &first, &last);
+                fwd_context32c ctx = {p, field, {0.0f, 0.0f}};
+                if (first <= last) traverse32c(entry, stepv, shape, first, last, forward_action32c, &ctx);
+                total = (double)ctx.total.sum - (double)ctx.total.carry;
+            } else {
+                blocksum_t acc = {0.0f, 0.0f, 0.0f};
+                for (int i = 0; i < S; ++i) {
+                    float q[3];
+                    point32c(entry, stepv, i, q);
+                    if (!finite3f(q)) status |= 2;
+                    blocksum_add(&acc, sample32c(p, field, q, shape, NULL, NULL), i, S);
+                }
+                total = (double)acc.sum - (double)acc.carry;
             }
             double step = (iv->upper - iv->lower) / (double)S;
-            integral = ((double)acc.sum - (double)acc.carry) * (ray->r.length * step);
+            integral = total * (ray->r.length * step);
         }
         *out = integral;
         if (!isfinite(p->image_dtype == DPT_F32 ? (double)(float)integral : integral)) status |= 2;
@@ -972,6 +1178,113 @@ static int flush_moments(const dpt_problem* p, moments_t* mo, float factor, doub
     return status;
 }
 
+/* F32C pose chain: clip-face seeds and the FP64 chain through M^T from the mean value,
+ * G = sum grad and H = sum alpha grad of one ray (alpha_i = (i + 0.5) / S). */
+static int pose_chain32c(const dpt_problem* p, const ray_t* ray, double seed, double span,
+                         double mean64, const double* Gd, const double* Hd, double* g12, double* g6)
+{
+    const interval64_t* iv = &ray->iv64;
+    int S = p->samples;
+    const double* d = ray->r.direction;
+    double g_along = fma(Gd[2], d[2], fma(Gd[1], d[1], Gd[0] * d[0]));
+    double h_along = fma(Hd[2], d[2], fma(Hd[1], d[1], Hd[0] * d[0]));
+    double shift_upper = h_along, shift_lower = g_along - h_along;
+    double lower_seed = fma(span, shift_lower, -mean64);
+    double upper_seed = fma(span, shift_upper, mean64);
+    double og[3], dg[3];
+    for (int a = 0; a < 3; ++a) {
+        double direct_direction = fma(span, Hd[a], iv->lower * Gd[a]);
+        og[a] = fma(upper_seed, iv->upper_origin[a],
+                    fma(lower_seed, iv->lower_origin[a], span * Gd[a]));
+        dg[a] = fma(upper_seed, iv->upper_direction[a],
+                    fma(lower_seed, iv->lower_direction[a], span * direct_direction));
+    }
+    double factor = seed * ray->r.length / (double)S;
+    double sa[3], da[3];
+    matvec_t(p->object_to_grid, og, sa);
+    matvec_t(p->object_to_grid, dg, da);
+    for (int a = 0; a < 3; ++a) {
+        sa[a] = factor * sa[a];
+        da[a] = factor * da[a];
+    }
+    if (g12) {
+        const double* wsr = ray->r.world_source_relative;
+        const double* wd = ray->r.world_direction;
+        for (int row = 0; row < 3; ++row)
+            for (int col = 0; col < 3; ++col)
+                g12[3 * row + col] = fma(wd[row], da[col], wsr[row] * sa[col]);
+        g12[12] = sa[0];
+        g12[13] = sa[1];
+        g12[14] = sa[2];
+    }
+    if (g6) {
+        const double* os = ray->r.object_source;
+        const double* od = ray->r.object_direction;
+        g6[0] = -sa[0];
+        g6[1] = -sa[1];
+        g6[2] = -sa[2];
+        g6[3] = fma(-da[2], od[1], da[1] * od[2]) + fma(-sa[2], os[1], sa[1] * os[2]);
+        g6[4] = fma(-da[0], od[2], da[2] * od[0]) + fma(-sa[0], os[2], sa[2] * os[0]);
+        g6[5] = fma(-da[1], od[0], da[0] * od[1]) + fma(-sa[1], os[0], sa[0] * os[1]);
+    }
+    return 0;
+}
+
+typedef struct {
+    const dpt_problem* p;
+    const void* field;
+    int active_volume, active_pose, status;
+    float volume_factor;
+    double* gradient;
+    kahan32_t mean;
+    float G[3], Hs[3];
+} vjp_context32c;
+
+/* One run of the segment form's VJP: the pose sums G = sum grad and Hs = sum (i + 0.5) grad
+ * and the compensated sum of the values, and the eight moments of the fractions expanded
+ * into the run cell's corner sums. */
+static void vjp_action32c(void* context, const run32c_t* r)
+{
+    vjp_context32c* ctx = (vjp_context32c*)context;
+    const float dx = r->d[0], dy = r->d[1], dz = r->d[2];
+    const float dxy = dx * dy, dxz = dx * dz, dyz = dy * dz;
+    const float nf = r->nf, s1 = r->s1, s2 = r->s2, s3 = r->s3;
+    if (ctx->active_pose) {
+        runpoly32c_t o;
+        run_poly32c(ctx->p, ctx->field, r, &o);
+        kahan_add32(&ctx->mean, run_sum32c(r, &o));
+        float g0[3] = {o.gx, o.gy, o.gz};
+        float g1[3] = {fmaf(o.t1, dz, o.a * dy), fmaf(o.t2, dz, o.a * dx), fmaf(o.t2, dy, o.t1 * dx)};
+        float g2[3] = {o.c[7] * dyz, o.c[7] * dxz, o.c[7] * dxy};
+        const float offset = (float)r->i0 + 0.5f;
+        for (int k = 0; k < 3; ++k) {
+            if (!r->interior[k]) g0[k] = g1[k] = g2[k] = 0.0f;
+            const float sg = fmaf(s2, g2[k], fmaf(s1, g1[k], nf * g0[k]));
+            const float sj = fmaf(s3, g2[k], fmaf(s2, g1[k], s1 * g0[k]));
+            ctx->G[k] = ctx->G[k] + sg;
+            ctx->Hs[k] = ctx->Hs[k] + fmaf(offset, sg, sj);
+        }
+    }
+    if (ctx->active_volume) {
+        const float fx = r->f[0], fy = r->f[1], fz = r->f[2];
+        const float fxy = fx * fy, fxz = fx * fz, fyz = fy * fz;
+        moments_t mo;
+        memcpy(mo.pending, r->cell, sizeof(mo.pending));
+        float* m = mo.m;
+        m[0] = nf;
+        m[1] = fmaf(s1, dx, nf * fx);
+        m[2] = fmaf(s1, dy, nf * fy);
+        m[3] = fmaf(s1, dz, nf * fz);
+        m[4] = fmaf(s2, dxy, fmaf(s1, fmaf(fx, dy, fy * dx), nf * fxy));
+        m[5] = fmaf(s2, dxz, fmaf(s1, fmaf(fx, dz, fz * dx), nf * fxz));
+        m[6] = fmaf(s2, dyz, fmaf(s1, fmaf(fy, dz, fz * dy), nf * fyz));
+        m[7] = fmaf(s3, dxy * dz,
+                    fmaf(s2, fmaf(fz, dxy, fmaf(fy, dxz, fx * dyz)),
+                         fmaf(s1, fmaf(fyz, dx, fmaf(fxz, dy, fxy * dz)), nf * (fxy * fz))));
+        ctx->status |= flush_moments(ctx->p, &mo, ctx->volume_factor, ctx->gradient);
+    }
+}
+
 /* One ray of the F32C VJP: FP64 clip and clip-face chain, FP32 marching, polynomial
  * values and slopes, blocked compensated mean, pose moments G = sum grad and
  * H = sum alpha grad, moment-based volume scatter. */
@@ -989,6 +1302,28 @@ static int vjp_ray_f32c(const dpt_problem* p, const void* field, const ray_t* ra
     float volume_factor = (float)(seed * ray->r.length * step);
     float entry[3], stepv[3];
     march32c(ray, S, entry, stepv);
+    if (moderate32c(entry, stepv)) {
+        int first, last;
+        inside_run32c(entry, stepv, shape, S, &first, &last);
+        vjp_context32c ctx;
+        memset(&ctx, 0, sizeof(ctx));
+        ctx.p = p;
+        ctx.field = field;
+        ctx.active_volume = active_volume;
+        ctx.active_pose = active_pose;
+        ctx.volume_factor = volume_factor;
+        ctx.gradient = sc->gradient;
+        if (first <= last) traverse32c(entry, stepv, shape, first, last, vjp_action32c, &ctx);
+        status |= ctx.status;
+        if (!active_pose) return status;
+        const double mean_seg = (double)ctx.mean.sum - (double)ctx.mean.carry;
+        double G_seg[3], H_seg[3];
+        for (int a = 0; a < 3; ++a) {
+            G_seg[a] = ctx.G[a];
+            H_seg[a] = (double)ctx.Hs[a] / (double)S;
+        }
+        return status | pose_chain32c(p, ray, seed, span, mean_seg, G_seg, H_seg, g12, g6);
+    }
     blocksum_t mean = {0.0f, 0.0f, 0.0f};
     float G[3] = {0}, H[3] = {0};
     float inv_s = 1.0f / (float)S;
@@ -1035,51 +1370,9 @@ static int vjp_ray_f32c(const dpt_problem* p, const void* field, const ray_t* ra
     }
     if (active_volume && mo.pending[0] >= 0) status |= flush_moments(p, &mo, volume_factor, sc->gradient);
     if (!active_pose) return status;
-    const double* d = ray->r.direction;
     double Gd[3] = {G[0], G[1], G[2]}, Hd[3] = {H[0], H[1], H[2]};
     double mean64 = (double)mean.sum - (double)mean.carry;
-    double g_along = fma(Gd[2], d[2], fma(Gd[1], d[1], Gd[0] * d[0]));
-    double h_along = fma(Hd[2], d[2], fma(Hd[1], d[1], Hd[0] * d[0]));
-    double shift_upper = h_along, shift_lower = g_along - h_along;
-    double lower_seed = fma(span, shift_lower, -mean64);
-    double upper_seed = fma(span, shift_upper, mean64);
-    double og[3], dg[3];
-    for (int a = 0; a < 3; ++a) {
-        double direct_direction = fma(span, Hd[a], iv->lower * Gd[a]);
-        og[a] = fma(upper_seed, iv->upper_origin[a],
-                    fma(lower_seed, iv->lower_origin[a], span * Gd[a]));
-        dg[a] = fma(upper_seed, iv->upper_direction[a],
-                    fma(lower_seed, iv->lower_direction[a], span * direct_direction));
-    }
-    double factor = seed * ray->r.length / (double)S;
-    double sa[3], da[3];
-    matvec_t(p->object_to_grid, og, sa);
-    matvec_t(p->object_to_grid, dg, da);
-    for (int a = 0; a < 3; ++a) {
-        sa[a] = factor * sa[a];
-        da[a] = factor * da[a];
-    }
-    if (g12) {
-        const double* wsr = ray->r.world_source_relative;
-        const double* wd = ray->r.world_direction;
-        for (int row = 0; row < 3; ++row)
-            for (int col = 0; col < 3; ++col)
-                g12[3 * row + col] = fma(wd[row], da[col], wsr[row] * sa[col]);
-        g12[12] = sa[0];
-        g12[13] = sa[1];
-        g12[14] = sa[2];
-    }
-    if (g6) {
-        const double* os = ray->r.object_source;
-        const double* od = ray->r.object_direction;
-        g6[0] = -sa[0];
-        g6[1] = -sa[1];
-        g6[2] = -sa[2];
-        g6[3] = fma(-da[2], od[1], da[1] * od[2]) + fma(-sa[2], os[1], sa[1] * os[2]);
-        g6[4] = fma(-da[0], od[2], da[2] * od[0]) + fma(-sa[0], os[2], sa[2] * os[0]);
-        g6[5] = fma(-da[1], od[0], da[0] * od[1]) + fma(-sa[1], os[0], sa[0] * os[1]);
-    }
-    return status;
+    return status | pose_chain32c(p, ray, seed, span, mean64, Gd, Hd, g12, g6);
 }
 
 /*
