@@ -589,26 +589,21 @@ struct CellRun {
     float nf, s1, s2, s3;  // n and the power sums of j over 0..n-1
 };
 
-__device__ __forceinline__ float plane_crossing(const float* entry, const float* inverse,
-                                                const float* sv, const int* axis_cell,
-                                                const int* shape, int k)
-{
-    if (sv[k] > 0.0f && axis_cell[k] + 1 <= shape[k] - 1)
-        return ((float)(axis_cell[k] + 1) - entry[k]) * inverse[k];
-    if (sv[k] < 0.0f && axis_cell[k] >= 0) return ((float)axis_cell[k] - entry[k]) * inverse[k];
-    return __int_as_float(0x7f800000);  // +inf: no plane left inside the support
-}
-
 // Walk the cell planes from sample `first` to `last` (sample i at entry + (i + 0.5) sv) and
 // call `action(run)` for every run with at least one sample.  Each step advances every axis
-// whose plane is the nearest, so the walk ends within nx + ny + nz + 3 steps.
+// whose plane is the nearest, so the walk ends within nx + ny + nz + 3 steps.  The plane an
+// axis meets next is kept as an exact float coordinate; it is crossed at sample coordinate
+// (plane - entry) / sv, computed as (plane - entry) * (1 / sv), or never (+inf) when it lies
+// outside the cell planes 0..n-1 or the ray does not move on that axis.
 template <typename Action>
 __device__ __forceinline__ void walk_cells(const FieldDims& dims, const float* entry, const float* sv,
                                            int first, int last, Action action)
 {
     const int shape[3] = {dims.nx, dims.ny, dims.nz};
-    float inverse[3], next[3];
-    int axis_cell[3];
+    const float top_plane[3] = {dims.mx, dims.my, dims.mz};  // n - 1
+    const float inf = __int_as_float(0x7f800000);
+    float inverse[3], next[3], plane[3], stepf[3];
+    int axis_cell[3], step[3];
     {
         const float offset = (float)first + 0.5f;
 #pragma unroll
@@ -616,16 +611,24 @@ __device__ __forceinline__ void walk_cells(const FieldDims& dims, const float* e
             const int c = (int)floorf(fmaf(offset, sv[k], entry[k]));
             axis_cell[k] = c < -1 ? -1 : (c > shape[k] - 1 ? shape[k] - 1 : c);
             inverse[k] = sv[k] != 0.0f ? 1.0f / sv[k] : 0.0f;
+            step[k] = sv[k] > 0.0f ? 1 : -1;
+            stepf[k] = (float)step[k];
+            plane[k] = (float)(axis_cell[k] + (sv[k] > 0.0f ? 1 : 0));
         }
     }
+    auto crossing = [&](int k) {
+        const bool valid = sv[k] != 0.0f && plane[k] >= 0.0f && plane[k] <= top_plane[k];
+        return valid ? (plane[k] - entry[k]) * inverse[k] : inf;
+    };
 #pragma unroll
-    for (int k = 0; k < 3; ++k) next[k] = plane_crossing(entry, inverse, sv, axis_cell, shape, k);
+    for (int k = 0; k < 3; ++k) next[k] = crossing(k);
+    const float end_limit = (float)(last + 1);
     int i = first;
     const int limit = shape[0] + shape[1] + shape[2] + 4;
     for (int walk = 0; walk < limit; ++walk) {
         const float nearest = fminf(next[0], fminf(next[1], next[2]));
         const float t = nearest - 0.5f;
-        const int end = !(t < (float)(last + 1)) ? last + 1 : (t <= (float)i ? i : (int)ceilf(t));
+        const int end = !(t < end_limit) ? last + 1 : (t <= (float)i ? i : (int)ceilf(t));
         if (end > i) {
             CellRun r;
             r.i0 = i;
@@ -636,25 +639,30 @@ __device__ __forceinline__ void walk_cells(const FieldDims& dims, const float* e
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int top = shape[k] - 2 < 0 ? 0 : shape[k] - 2;
-                if (axis_cell[k] >= 0 && axis_cell[k] <= shape[k] - 2) {
-                    lower[k] = axis_cell[k];
-                    r.f[k] = fmaf(offset, sv[k], entry[k]) - (float)axis_cell[k];
-                    r.d[k] = sv[k];
-                    r.interior |= 1 << k;
-                } else {
-                    lower[k] = axis_cell[k] < 0 ? 0 : top;
-                    r.f[k] = (axis_cell[k] < 0 || shape[k] == 1) ? 0.0f : 1.0f;
-                    r.d[k] = 0.0f;
-                }
+                const bool interior = axis_cell[k] >= 0 && axis_cell[k] <= shape[k] - 2;
+                lower[k] = interior ? axis_cell[k] : (axis_cell[k] < 0 ? 0 : top);
+                const float margin = (axis_cell[k] < 0 || shape[k] == 1) ? 0.0f : 1.0f;
+                r.f[k] = interior ? fmaf(offset, sv[k], entry[k]) - (float)axis_cell[k] : margin;
+                r.d[k] = interior ? sv[k] : 0.0f;
+                r.interior |= interior ? 1 << k : 0;
             }
             r.lx = lower[0];
             r.ly = lower[1];
             r.lz = lower[2];
             r.cell = (lower[2] * dims.ny + lower[1]) * dims.nx + lower[0];
-            const int64_t m = r.n;
-            r.nf = (float)m;
-            r.s1 = (float)(m * (m - 1) / 2);
-            r.s2 = (float)(m * (m - 1) * (2 * m - 1) / 6);
+            // power sums of j = 0..n-1 (exact integers, rounded once to FP32); 32-bit
+            // arithmetic is exact up to n = 1024
+            if (r.n <= 1024) {
+                const unsigned m = (unsigned)r.n;
+                const unsigned s1 = m * (m - 1u) / 2u;
+                r.s1 = (float)s1;
+                r.s2 = (float)(s1 * (2u * m - 1u) / 3u);
+            } else {
+                const int64_t m = r.n;
+                r.s1 = (float)(m * (m - 1) / 2);
+                r.s2 = (float)(m * (m - 1) * (2 * m - 1) / 6);
+            }
+            r.nf = (float)r.n;
             r.s3 = r.s1 * r.s1;
             action(r);
         }
@@ -663,8 +671,9 @@ __device__ __forceinline__ void walk_cells(const FieldDims& dims, const float* e
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             if (next[k] == nearest) {
-                axis_cell[k] += sv[k] > 0.0f ? 1 : -1;
-                next[k] = plane_crossing(entry, inverse, sv, axis_cell, shape, k);
+                axis_cell[k] += step[k];
+                plane[k] += stepf[k];
+                next[k] = crossing(k);
             }
         }
     }

@@ -20,15 +20,23 @@
 #include "launch.h"
 
 // DPT_VJP_REUSE=1 keeps the last cell's values across samples (fewer loads, one more branch
-// per sample: 3% slower measured); DPT_VJP_MIN_BLOCKS bounds registers for that many
-// resident blocks (spills at 3 x 256 threads).
+// per sample: 3% slower measured).
 #ifndef DPT_VJP_REUSE
 #define DPT_VJP_REUSE 0
 #endif
-#ifdef DPT_VJP_MIN_BLOCKS
-#define DPT_VJP_BOUNDS __launch_bounds__(kVjpBlock, DPT_VJP_MIN_BLOCKS)
-#else
-#define DPT_VJP_BOUNDS __launch_bounds__(kVjpBlock)
+// Resident blocks per SM the register allocation must allow, per arithmetic (128-thread
+// blocks).  The kernels are latency bound, so occupancy pays for a few spilled registers:
+// the compensated form's cell walk measured 0.71 ms per 512^2 view (S = 1024) at four
+// blocks (118 registers), 0.59 at eight (64 registers, 376 bytes spilled to L1); the FP32
+// form 1.17 ms at five blocks (96 registers), 1.15 at six (80 registers, 12 bytes spilled).
+#ifndef DPT_VJP_MIN_BLOCKS_F32
+#define DPT_VJP_MIN_BLOCKS_F32 6
+#endif
+#ifndef DPT_VJP_MIN_BLOCKS_F32C
+#define DPT_VJP_MIN_BLOCKS_F32C 8
+#endif
+#ifndef DPT_VJP_MIN_BLOCKS_F64
+#define DPT_VJP_MIN_BLOCKS_F64 3
 #endif
 
 namespace dpt {
@@ -91,7 +99,7 @@ __device__ __forceinline__ void pose_epilogue(const RayArgs& a, const ViewShared
 }
 
 template <int kArith, class Field, bool kVol, bool kPose, typename Seed>
-__global__ void DPT_VJP_BOUNDS k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
+__global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_MIN_BLOCKS_F32C : kArith == DPT_ARITH_F32 ? DPT_VJP_MIN_BLOCKS_F32 : DPT_VJP_MIN_BLOCKS_F64) k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
                                                 int mode, float* __restrict__ acc,
                                                 double* __restrict__ partials)
 {

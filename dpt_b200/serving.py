@@ -176,6 +176,7 @@ class _Job:
     event: Any = None
     outputs: dict = field(default_factory=dict)
     workspace: Any = None
+    key: Any = None  # request class: volume, geometry, samples, precision, kind
 
 
 class _Slot:
@@ -188,6 +189,7 @@ class _Slot:
         self.stream = torch.cuda.Stream(device=device) if stream is None else stream
         self.workspaces: OrderedDict[Any, Any] = OrderedDict()
         self.graphs: dict[Any, Any] = {}
+        self.classes: set[Any] = set()  # request classes whose workspace (and graph) this slot holds
         self.busy = False
         self._pinned: dict[str, Any] = {}
 
@@ -264,9 +266,13 @@ class ProjectionServer:
     def submit(self, request: ProjectionRequest) -> Future:
         if request.volume not in self.volumes:
             raise ContractError(f"unknown volume {request.volume!r}")
+        from .plan import batched
+
         future: Future = Future()
         job = _Job(request, future, time.perf_counter())
         job.nbytes = self.request_bytes(request)
+        job.key = (request.volume, batched(request.geometry), request.samples_per_ray, request.precision,
+                   request.kind)
         with self.lock:
             if self.closed:
                 raise ContractError("server is closed")
@@ -326,8 +332,12 @@ class ProjectionServer:
                     return
                 free = [slot for slot in self.slots if not slot.busy]
                 taken = self.admission.take(len(free))
-                for (job, _), slot in zip(taken, free, strict=False):
+                for job, _ in taken:
+                    # prefer a free slot that already holds this class's workspace and graph
+                    slot = next((s for s in free if job.key in s.classes), free[0])
+                    free.remove(slot)
                     slot.busy = True
+                    slot.classes.add(job.key)
                     job.slot = slot
             for job, _ in taken:
                 try:
@@ -397,6 +407,7 @@ class ProjectionServer:
                 evicted, _ = slot.workspaces.popitem(last=False)
                 # a captured graph points into its workspace's scratch: drop them together
                 slot.graphs.pop(evicted, None)
+                slot.classes.discard(evicted[:5])
         else:
             slot.workspaces.move_to_end(key)
         return key, found
@@ -476,6 +487,10 @@ class ProjectionServer:
             status_host.copy_(ws.status, non_blocking=True)
             ws.status.zero_()
             job.outputs = dict(outputs, status=status_host)
+            if "loss" in outputs:  # read back with the status, no host synchronisation later
+                loss_host = slot.pinned("loss", 1, torch.float64)
+                loss_host.copy_(outputs["loss"].reshape(1), non_blocking=True)
+                job.outputs["loss_host"] = loss_host
             job.workspace = ws
             job.event = torch.cuda.Event()
             job.event.record(slot.stream)
@@ -512,7 +527,8 @@ class ProjectionServer:
                   "target": None if inputs["target"] is None else inputs["target"].clone()}
         graph = torch.cuda.CUDAGraph()
         slot.stream.synchronize()
-        with torch.cuda.graph(graph, stream=slot.stream):
+        # thread-local capture: the completion thread may read finished results meanwhile
+        with torch.cuda.graph(graph, stream=slot.stream, capture_error_mode="thread_local"):
             outputs = self._body(ws, field_tensor, static, request)
         ws.status.zero_()
         slot.graphs[key] = (graph, static, outputs)
@@ -529,10 +545,10 @@ class ProjectionServer:
                 except (ContractError, NumericalError) as error:
                     error.args = (f"projection view {view}: {error}", *error.args[1:])
                     raise
-        loss = outputs.get("loss")
+        loss = outputs.get("loss_host")
         return ProjectionResult(
             image=outputs["image"],
-            loss=None if loss is None else float(loss),
+            loss=None if loss is None else float(loss[0]),
             volume_gradient=outputs.get("volume_gradient"),
             pose_gradient=outputs.get("pose_gradient"),
             submitted=job.submitted,
