@@ -61,6 +61,7 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--mode", choices=("iteration", "serving", "precision"), default="iteration",
                         help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
     parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
+    parser.add_argument("--slots", type=int, default=4, help="serving mode: concurrent request streams")
     return parser.parse_args()
 
 
@@ -470,10 +471,11 @@ def serving_requests(args, device):
 
 
 def run_serving(args) -> None:
-    """Served mixed stream against the same requests run one after another.
+    """Served mixed stream against the same requests run one after another through the plain
+    FP32 projector (and, for reference, through the server's own launch sequence alone).
 
     Capacity: every request submitted at once, time until the last completes (the server
-    overlaps requests on its slots' streams), against back-to-back calls on one stream.
+    overlaps requests on its slots' streams).
     Latency: Poisson arrivals at 70% of the measured served capacity, p50/p99 from submit
     to result."""
     import numpy as np
@@ -491,7 +493,45 @@ def run_serving(args) -> None:
         results = [future.result() for future in futures]
         return max(r.finished for r in results) - start
 
-    with ProjectionServer(str(device), slots=4) as server:
+    # sequential plain calls: each request through the public FP32 Projector (autograd for
+    # the gradients), one after another, each result read before the next call
+    from dpt_b200.torch import Projector
+    from dpt_b200.torch import _projection_ops as ops
+
+    ops.set_cache_limit(4 * len(stream))  # every request's plan and field copy stays warm
+    fields32 = {name: torch.tensor(values, device=device) for name, (_, values) in volumes.items()}
+    modules = [Projector(grid=volumes[name][0], geometry=request.geometry, precision="fp32",
+                         samples_per_ray=request.samples_per_ray) for request, _, name in stream]
+
+    def plain(k: int) -> float:
+        request, _, name = stream[k]
+        field = fields32[name]
+        if request.kind == "forward":
+            with torch.no_grad():
+                return float(modules[k](field).sum())
+        if request.kind == "volume":
+            f = field.detach().requires_grad_(True)
+            image = modules[k](f)
+            loss = 0.5 * (image.double() * image.double()).sum()
+            loss.backward()
+            return float(loss) + float(f.grad.reshape(-1)[0])
+        tangent = torch.zeros(6, dtype=torch.float64, device=device, requires_grad=True)
+        image = modules[k](field, tangent)
+        loss = 0.5 * (image.double() * image.double()).sum()
+        loss.backward()
+        return float(loss) + float(tangent.grad[0])
+
+    for k in range(len(stream)):  # warm-up: workspaces, field copies
+        plain(k)
+    torch.cuda.synchronize()
+    start = time.perf_counter()
+    for k in range(len(stream)):
+        plain(k)
+    torch.cuda.synchronize()
+    sequential_s = time.perf_counter() - start
+    del modules
+
+    with ProjectionServer(str(device), slots=args.slots) as server:
         for name, (grid, values) in volumes.items():
             for storage in ("float32", "bfloat16"):
                 server.add_volume(f"{name}:{storage}", grid, values, storage=storage)
@@ -502,7 +542,7 @@ def run_serving(args) -> None:
         for request in requests:
             server.run_alone(request)
         torch.cuda.synchronize()
-        sequential_s = time.perf_counter() - start
+        alone_s = time.perf_counter() - start
         for _ in range(2):  # warm the served path: workspaces, tiles and graphs on the slots
             saturated(server)
         served_s = min(saturated(server) for _ in range(3))
@@ -526,6 +566,8 @@ def run_serving(args) -> None:
         "unit": "requests/s",
         "sequential_requests_per_s": len(requests) / sequential_s,
         "speedup_vs_sequential": sequential_s / served_s,
+        "sequential_same_arithmetic_requests_per_s": len(requests) / alone_s,
+        "speedup_vs_sequential_same_arithmetic": alone_s / served_s,
         "p50_ms": percentile(latencies, 50),
         "p99_ms": percentile(latencies, 99),
         "latency_load_requests_per_s": rate,
@@ -535,9 +577,14 @@ def run_serving(args) -> None:
         "higher_is_better": True,
         "config": {"workload": "Poisson mix: 64^3/128^3/256^3/512x512x128 volumes FP32|BF16, 1-64 views, "
                                "128^2-1024^2 detectors, S 128-1024, 60/30/10 forward/volume/pose",
+                   "sequential": "plain FP32 Projector calls (FP32 copies of the BF16 volumes), one "
+                                 "after another, each result read before the next call",
+                   "sequential_same_arithmetic": "the server's own launch sequence per request, one "
+                                                 "after another on one stream (BF16 volumes in the "
+                                                 "compensated form)",
                    "capacity": "all requests submitted at once, best of 3 after 2 warm rounds",
                    "latency": "Poisson arrivals at 70% of served capacity, 4 rounds",
-                   "slots": 4, "memory_budget_gib": 120},
+                   "slots": args.slots, "memory_budget_gib": 120},
     }
     print(json.dumps(line), flush=True)
 

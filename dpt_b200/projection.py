@@ -128,10 +128,79 @@ def _stream(device: torch.device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
 
 
-class ProjectionWorkspace:
-    """Device state of one (grid, geometry, spec) on one CUDA device."""
+class FieldCopies:
+    """Field copies (the replicated or polynomial sampling layout) shared by every workspace
+    on one device that samples the same field with the same layout, so that many request
+    classes over one resident volume hold one copy instead of one each.
 
-    def __init__(self, plan: RayPlan, spec: ProjectionSpec, device: torch.device | str) -> None:
+    An entry is keyed by the field's storage pointer, its version counter and the layout; it
+    lives while the field does.  A workspace that finds the copy written on another stream
+    waits for the event recorded after the write before it samples the copy.
+    """
+
+    def __init__(self) -> None:
+        self._entries: dict[tuple, tuple] = {}
+        self._lock = threading.Lock()
+
+    def lookup(self, key: tuple, field: torch.Tensor):
+        with self._lock:
+            entry = self._entries.get(key)
+            if entry is None:
+                return None
+            ref, tensor, event = entry
+            if ref() is not field:
+                del self._entries[key]
+                return None
+            return tensor, event
+
+    def store(self, key: tuple, field: torch.Tensor, tensor: torch.Tensor, event) -> None:
+        with self._lock:
+            # drop copies of dead fields and older versions of this one (same pointer, layout)
+            for stale in [k for k, (ref, _, _) in self._entries.items()
+                          if ref() is None or (k[0] == key[0] and k[2:] == key[2:])]:
+                del self._entries[stale]
+            self._entries[key] = (weakref.ref(field), tensor, event)
+
+    def bytes(self) -> int:
+        with self._lock:
+            return sum(t.numel() * t.element_size() for _, t, _ in self._entries.values())
+
+
+class ScratchPool:
+    """Volume-gradient scratch (the 32-byte corner-sum records and the FP64 running total)
+    shared by workspaces that never run at the same time, e.g. the request classes of one
+    serving stream: one buffer per voxel count instead of one per workspace.  The records
+    are left zeroed by every fold, so a workspace can take over the buffer another left."""
+
+    def __init__(self, device: torch.device | str) -> None:
+        self.device = torch.device(device)
+        self._accumulators: dict[int, torch.Tensor] = {}
+        self._totals: dict[int, torch.Tensor] = {}
+
+    def accumulator(self, floats: int) -> torch.Tensor:
+        found = self._accumulators.get(floats)
+        if found is None:
+            found = torch.zeros(floats, dtype=torch.float32, device=self.device)
+            self._accumulators[floats] = found
+        return found
+
+    def total(self, voxels: int) -> torch.Tensor:
+        found = self._totals.get(voxels)
+        if found is None:
+            found = torch.empty(voxels, dtype=torch.float64, device=self.device)
+            self._totals[voxels] = found
+        return found
+
+
+class ProjectionWorkspace:
+    """Device state of one (grid, geometry, spec) on one CUDA device.
+
+    ``copies`` (a FieldCopies) shares the field's sampling copy with other workspaces;
+    ``pool`` (a ScratchPool) shares the volume-gradient scratch with workspaces that never
+    run concurrently with this one."""
+
+    def __init__(self, plan: RayPlan, spec: ProjectionSpec, device: torch.device | str, *,
+                 copies: FieldCopies | None = None, pool: ScratchPool | None = None) -> None:
         device = torch.device(device)
         if device.type != "cuda":
             raise ContractError("the B200 projector runs on CUDA devices only")
@@ -142,6 +211,8 @@ class ProjectionWorkspace:
         self.spec = spec
         self.device = device
         self.lock = threading.RLock()
+        self.copies = copies
+        self.pool = pool
         self.problem = plan.problem(
             spec.samples_per_ray,
             spec.arith,
@@ -194,12 +265,18 @@ class ProjectionWorkspace:
     def accumulator(self) -> torch.Tensor:
         if self._accumulator is None:
             size = N.library().dpt_b200_accumulator_bytes(self.problem)
-            self._accumulator = torch.zeros(size // 4, dtype=torch.float32, device=self.device)
+            if self.pool is not None:
+                self._accumulator = self.pool.accumulator(size // 4)
+            else:
+                self._accumulator = torch.zeros(size // 4, dtype=torch.float32, device=self.device)
         return self._accumulator
 
     def total(self) -> torch.Tensor:
         if self._total is None:
-            self._total = torch.empty(self.plan.grid.voxels, dtype=torch.float64, device=self.device)
+            if self.pool is not None:
+                self._total = self.pool.total(self.plan.grid.voxels)
+            else:
+                self._total = torch.empty(self.plan.grid.voxels, dtype=torch.float64, device=self.device)
         return self._total
 
     def partials(self) -> torch.Tensor:
@@ -257,11 +334,28 @@ class ProjectionWorkspace:
                                                _stream(self.device)))
                 return self._packed
         size = lib.dpt_b200_packed_bytes(self.problem)
+        key = (field.data_ptr(), field._version, self.problem.arith == N.ARITH_F32C, size)
+        if self.copies is not None:
+            found = self.copies.lookup(key, field)
+            if found is not None:
+                copy, event = found
+                torch.cuda.current_stream(self.device).wait_event(event)
+                self._run("prepare_field", lambda: lib.dpt_b200_prepare_field(
+                    self.problem, field.data_ptr(), None, poses.data_ptr(), self.status.data_ptr(),
+                    _stream(self.device)))
+                self._packed = copy
+                self._packed_for = (weakref.ref(field), field._version, field.data_ptr())
+                return copy
+            self._packed = None  # never write into a copy other workspaces share
         if self._packed is None or self._packed.numel() < size:
             self._packed = self._bytes(size)
         self._run("prepare_field", lambda: lib.dpt_b200_prepare_field(self.problem, field.data_ptr(), self._packed.data_ptr(),
                                        poses.data_ptr(), self.status.data_ptr(), _stream(self.device)))
         self._packed_for = (weakref.ref(field), field._version, field.data_ptr())
+        if self.copies is not None:
+            event = torch.cuda.Event()
+            event.record(torch.cuda.current_stream(self.device))
+            self.copies.store(key, field, self._packed, event)
         return self._packed
 
     # ----------------------------------------------------------- launches

@@ -11,7 +11,9 @@ adds on top of the projector:
   waiting for memory does not block small ones behind it);
 * every admitted request runs on its own CUDA stream, so requests that arrive while
   others are on the GPU overlap on the device;
-* repeated request shapes replay a captured CUDA graph of their launch sequence;
+* repeated request shapes below ``graph_samples`` nominal ray-samples replay a captured
+  CUDA graph of their launch sequence (larger requests are launch-count bound no more, and
+  a replay must copy its outputs out of the graph's static buffers);
 * the detector tile of each request class comes from a small autotuner that times the
   candidate tiles once per class and keeps the fastest.
 
@@ -32,6 +34,7 @@ from dataclasses import dataclass, field
 from typing import Any, Literal
 
 from .contracts import ContractError, integer
+from .projection import FieldCopies, ScratchPool
 
 RequestKind = Literal["forward", "volume", "pose"]
 
@@ -189,6 +192,7 @@ class _Slot:
         self.stream = torch.cuda.Stream(device=device) if stream is None else stream
         self.workspaces: OrderedDict[Any, Any] = OrderedDict()
         self.graphs: dict[Any, Any] = {}
+        self.pool = ScratchPool(device)  # gradient scratch shared by this slot's workspaces
         self.classes: set[Any] = set()  # request classes whose workspace (and graph) this slot holds
         self.busy = False
         self._pinned: dict[str, Any] = {}
@@ -214,7 +218,8 @@ class ProjectionServer:
     """
 
     def __init__(self, device: str = "cuda:0", *, memory_budget_bytes: int = 120 << 30, slots: int = 4,
-                 graphs: bool = True, autotune: bool = True, workspaces_per_slot: int = 8) -> None:
+                 graphs: bool = True, autotune: bool = True, workspaces_per_slot: int = 64,
+                 graph_samples: int = 1 << 30) -> None:
         import torch
 
         self.torch = torch
@@ -226,9 +231,12 @@ class ProjectionServer:
         self.admission = Admission(memory_budget_bytes)
         self.tuner = TileTuner()
         self.graphs = graphs
+        self.graph_samples = graph_samples
         self.autotune = autotune
         self.workspaces_per_slot = workspaces_per_slot
         self.volumes: dict[str, _Volume] = {}
+        # one sampling copy per resident volume and layout, shared by all slots and classes
+        self.copies = FieldCopies()
         self._alone: _Slot | None = None
         self._identity: dict[int, Any] = {}
         self.lock = threading.Condition()
@@ -306,6 +314,12 @@ class ProjectionServer:
         self.close()
 
     # ---------------------------------------------------------- sizing
+    def _small(self, request: ProjectionRequest) -> bool:
+        """Whether a request is small enough for graph replay to pay (nominal ray-samples)."""
+        from .plan import batched
+
+        return batched(request.geometry).pixels * request.samples_per_ray < self.graph_samples
+
     def request_bytes(self, request: ProjectionRequest) -> int:
         from .plan import batched
 
@@ -315,9 +329,10 @@ class ProjectionServer:
         image = 8 if request.precision == "fp64" else 4
         total = 3 * rays * image + 4096
         voxels = volume.grid.voxels
-        total += voxels * 16  # replicated field copy of this slot's workspace
+        # the field copy and the slot's gradient scratch are shared and counted once, when
+        # the volume is added; a request needs its images, gradient and pose partials
         if request.kind == "volume":
-            total += voxels * (32 + 8 + 4)
+            total += voxels * 4
         if request.kind == "pose":
             total += len(geometry.views) * ((rays // len(geometry.views)) // 256 + 1) * 96 + 96 * rays // 256
         return total
@@ -342,7 +357,7 @@ class ProjectionServer:
             for job, _ in taken:
                 try:
                     job.started = time.perf_counter()
-                    self._launch(job, use_graph=self.graphs)
+                    self._launch(job, use_graph=self.graphs and self._small(job.request))
                 except BaseException as error:  # surfaced through the future
                     job.outputs["error"] = error
                     job.event = None
@@ -401,7 +416,8 @@ class ProjectionServer:
                                   precision="float64" if request.precision == "fp64" else "float32",
                                   sampling_precision=sampling, storage_precision=storage,
                                   block_cols=block_cols)
-            found = ProjectionWorkspace(plan_rays(volume.grid, geometry), spec, self.device)
+            found = ProjectionWorkspace(plan_rays(volume.grid, geometry), spec, self.device,
+                                        copies=self.copies, pool=slot.pool)
             slot.workspaces[key] = found
             while len(slot.workspaces) > self.workspaces_per_slot:
                 evicted, _ = slot.workspaces.popitem(last=False)

@@ -32,7 +32,7 @@ from threading import RLock
 
 import torch
 
-from ..contracts import ContractError
+from ..contracts import ContractError, integer
 from ..geometry import BatchedGeometry, CurvedDetectorGeometry, DetectorGeometry, ParallelGeometry
 from ..projection import ProjectionSpec, ProjectionWorkspace
 from ..plan import plan_rays
@@ -116,6 +116,18 @@ def workspace(field: torch.Tensor, value: str, active_volume: bool, active_pose:
         while len(_CACHE) > _CACHE_LIMIT:
             _CACHE.popitem(last=False)
         return found
+
+
+def set_cache_limit(limit: int) -> None:
+    """Keep up to ``limit`` workspaces (plans, field copies, scratch) across calls; the least
+    recently used beyond it are released.  The default, 8, suits one training loop; callers
+    cycling through many configurations keep their state warm with a larger limit."""
+    global _CACHE_LIMIT
+    integer(limit, "limit", minimum=1)
+    with _CACHE_LOCK:
+        _CACHE_LIMIT = limit
+        while len(_CACHE) > _CACHE_LIMIT:
+            _CACHE.popitem(last=False)
 
 
 def clear_cache() -> None:

@@ -135,3 +135,40 @@ def test_budget_limits_concurrency():
     assert len(results) == len(requests)
     assert server.admission.peak <= largest
     assert server.admission.in_use == 0
+
+
+@pytest.mark.gpu
+def test_shared_field_copies_and_scratch_pool_match_private_workspaces():
+    import torch
+
+    from dpt_b200.plan import plan_rays
+    from dpt_b200.projection import FieldCopies, ProjectionSpec, ProjectionWorkspace, ScratchPool
+
+    scenes, intrinsics_type = _scenes()
+    grid, values = scenes["mid"]
+    field = torch.tensor(values, device="cuda:0")
+    copies, pool = FieldCopies(), ScratchPool("cuda:0")
+    geometries = [intrinsics_type(120.0, 200.0, (n, n), (1.6, 1.6)).batch((0.1 * n, 0.2 * n)) for n in (16, 24)]
+    for sampling in ("float32", "compensated"):
+        spec = ProjectionSpec(40, sampling_precision=sampling, active_volume=True)
+        private = [ProjectionWorkspace(plan_rays(grid, g), spec, "cuda:0") for g in geometries]
+        shared = [ProjectionWorkspace(plan_rays(grid, g), spec, "cuda:0", copies=copies, pool=pool)
+                  for g in geometries]
+        poses = torch.tensor((1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0, 0, 0, 0), dtype=torch.float64, device="cuda:0")
+        side = torch.cuda.Stream()
+        for round_ in range(2):
+            if round_ == 1:
+                field.mul_(1.5)  # in-place change: every copy must be rewritten
+            for p, s in zip(private, shared, strict=True):
+                poses_v = poses.expand(p.views, 12).contiguous()
+                expected = p.forward(field, poses_v)
+                with torch.cuda.stream(side):  # the shared copy is written on another stream
+                    side.wait_stream(torch.cuda.current_stream())
+                    got = s.forward(field, poses_v)
+                torch.cuda.current_stream().wait_stream(side)
+                torch.testing.assert_close(got, expected, rtol=0, atol=0)
+                cot = torch.full_like(expected, 0.25)
+                g_expected, _ = p.vjp(field, poses_v, cot, volume=True, pose=None)
+                g_got, _ = s.vjp(field, poses_v, cot, volume=True, pose=None)
+                assert torch.linalg.norm(g_got - g_expected) <= 1e-6 * torch.linalg.norm(g_expected)
+        assert copies.bytes() > 0
