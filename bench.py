@@ -339,6 +339,11 @@ def run_gpu(args) -> None:
                 "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dominant,
                 "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
                 "l2_peak": round(l2, 1), "frac_l2": round(achieved / l2, 4),
+                # the whole iteration (forward + joint VJP: 16 b_s + 32 bytes per realised
+                # sample) over the device-timed step, against the measured L2 copy bandwidth
+                "iteration": {"bytes_per_sample": 16 * storage_bytes + 32,
+                              "achieved": round((16 * storage_bytes + 32) * realised / (step_ms * 1e-3) / 1e9, 1),
+                              "frac_l2": round((16 * storage_bytes + 32) * realised / (step_ms * 1e-3) / 1e9 / l2, 4)},
                 "l2_peak_source": "measured here: copy of a 2 x 32 MiB L2-resident buffer, best of 5 x 50",
                 "kernel_ms": {k: round(v / args.steps, 3) for k, v in sorted(totals.items())}}
 

@@ -15,11 +15,12 @@ from pathlib import Path
 from .contracts import ContractError
 
 LIBRARY_PATH = Path(__file__).resolve().parent / "_lib" / "libdpt_b200.so"
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # Mirrors of the header's enums.
 F32, F64, F16, BF16 = 0, 1, 2, 3
-ARITH_F32, ARITH_F64, ARITH_F32C = 0, 1, 2
+ARITH_F32, ARITH_F64, ARITH_F32C, ARITH_MIXED, ARITH_FAST, ARITH_CELLS = 0, 1, 2, 3, 4, 5
+DOMAIN_PHYSICAL, DOMAIN_SIGNED = 0, 1
 RAYS_PANELS, RAYS_BUNDLE = 0, 1
 PANEL_CONE, PANEL_PARALLEL, PANEL_CURVED = 0, 1, 2
 VIEW_WORDS, VIEW_MODE_WORD = 20, 18
@@ -61,6 +62,8 @@ class Problem(ctypes.Structure):
         ("image_dtype", ctypes.c_int32),
         ("layout", ctypes.c_int32),
         ("block_cols", ctypes.c_int32),
+        ("field_domain", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
         ("object_to_grid", ctypes.c_double * 9),
         ("grid_origin", ctypes.c_double * 3),
     ]

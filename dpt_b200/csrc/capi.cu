@@ -77,17 +77,19 @@ int check_problem(const dpt_problem* p)
     if (p->image_dtype != DPT_F32 && p->image_dtype != DPT_F64) return DPT_E_DTYPE;
     if (p->field_dtype != DPT_F32 && p->field_dtype != DPT_F16 && p->field_dtype != DPT_BF16)
         return DPT_E_DTYPE;
-    if (p->arith != DPT_ARITH_F32 && p->arith != DPT_ARITH_F64 && p->arith != DPT_ARITH_F32C)
-        return DPT_E_DTYPE;
-    // FP32 and FP64 sample arithmetic read FP32 storage; FP16/BF16 storage uses F32C.
-    if (p->field_dtype != DPT_F32 && p->arith != DPT_ARITH_F32C) return DPT_E_DTYPE;
+    if (p->arith < DPT_ARITH_F32 || p->arith > DPT_ARITH_CELLS) return DPT_E_DTYPE;
+    // the reference FP32 arithmetic reads FP32 storage (reference ProjectionSpec rule); the
+    // others decode FP16/BF16 values in the pack kernel
+    if (p->field_dtype != DPT_F32 && p->arith == DPT_ARITH_F32) return DPT_E_DTYPE;
+    if (p->field_domain != DPT_DOMAIN_PHYSICAL && p->field_domain != DPT_DOMAIN_SIGNED) return DPT_E_FLAGS;
     if (p->layout != DPT_LAYOUT_REPLICATED && p->layout != DPT_LAYOUT_DIRECT) return DPT_E_FLAGS;
     if (p->layout == DPT_LAYOUT_DIRECT && p->field_dtype != DPT_F32) return DPT_E_DTYPE;
     if (p->block_cols != 0 && p->block_cols != 8 && p->block_cols != 16 && p->block_cols != 32 &&
         p->block_cols != 64)
         return DPT_E_FLAGS;
     // FP32 grid coordinates are exact integers only up to 2^24 (reference projection.py:548).
-    if (p->arith != DPT_ARITH_F64 && (p->nx > (1 << 24) || p->ny > (1 << 24) || p->nz > (1 << 24)))
+    if (p->arith != DPT_ARITH_F64 && p->arith != DPT_ARITH_CELLS &&
+        (p->nx > (1 << 24) || p->ny > (1 << 24) || p->nz > (1 << 24)))
         return DPT_E_SHAPE;
     return DPT_OK;
 }
@@ -207,6 +209,8 @@ int dpt_b200_vjp(const dpt_problem* p, const dpt_rays* r, const void* packed,
     if (!(flags & DPT_VJP_VOLUME) && !pose_bits) return DPT_E_FLAGS;
     if (pose_bits && (pose_bits & (pose_bits - 1))) return DPT_E_FLAGS;  // one pose form
     if ((flags & DPT_VJP_PER_RAY6) && (flags & DPT_VJP_VOLUME)) return DPT_E_FLAGS;
+    // the mixed and fast samplings are fixed-pose forms (reference ProjectionSpec rule)
+    if (pose_bits && (p->arith == DPT_ARITH_MIXED || p->arith == DPT_ARITH_FAST)) return DPT_E_FLAGS;
     if ((flags & DPT_VJP_VOLUME) && !accumulator) return DPT_E_NULL;
     if (accumulator && !aligned(accumulator, 32)) return DPT_E_ALIGN;
     if (pose_bits && !pose_partials) return DPT_E_NULL;

@@ -727,6 +727,138 @@ struct Kahan32 {
     __device__ __forceinline__ double value() const { return (double)sum - (double)carry; }
 };
 
+// ------------------------------------------------------ FP64 cell-Gauss integration
+//
+// Reference kernels/projection.py:522-746: the clipped ray is split at every interpolation
+// plane (integer grid coordinates 0..n-1; the half-cell margins are segments of their own)
+// and each segment, on which the trilinear field is a cubic in the ray parameter, is
+// integrated exactly with the two-node Gauss rule.  The arithmetic follows the reference
+// step for step (the FMA-corrected reciprocal crossings, ties advanced together), so the
+// segments and nodes are the reference's.
+
+// Strict FP64 sample (reference sample_field / sample_cell_fraction): zero outside the
+// half-cell support; the value and, when `g` is given, the slope-masked grid gradient.
+template <class Field>
+__device__ __forceinline__ double sample_strict64(const Field& f, const FieldDims& d, const double* p,
+                                                  double* g)
+{
+    if (g) g[0] = g[1] = g[2] = 0.0;
+    if (!inside(p[0], p[1], p[2], d.nx, d.ny, d.nz)) return 0.0;
+    const double mx = (double)(d.nx - 1), my = (double)(d.ny - 1), mz = (double)(d.nz - 1);
+    const Axis64 X = axis64(p[0], mx, d.cx), Y = axis64(p[1], my, d.cy), Z = axis64(p[2], mz, d.cz);
+    float v32[8];
+    f.load_at((Z.lower * d.ny + Y.lower) * d.nx + X.lower, X.lower, Y.lower, Z.lower, v32);
+    double v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = (double)v32[c];
+    if (g) {
+        const double sx = (p[0] >= 0.0 && p[0] < mx) ? 1.0 : 0.0;
+        const double sy = (p[1] >= 0.0 && p[1] < my) ? 1.0 : 0.0;
+        const double sz = (p[2] >= 0.0 && p[2] < mz) ? 1.0 : 0.0;
+        slope64(X.fraction, Y.fraction, Z.fraction, v, sx, sy, sz, g);
+    }
+    return interpolate64(X.fraction, Y.fraction, Z.fraction, v);
+}
+
+struct GaussSegment {
+    double end, radius, first_position, second_position;
+    double first[3], second[3];  // the two Gauss nodes
+    int lower[3];                // interpolation cell of the segment centre
+    bool shared;                 // both nodes in that cell (one combined scatter)
+};
+
+struct CellWalk64 {
+    int plane[3], step[3];
+    double next[3], inverse[3];
+
+    // reference crossing_quotient (:530-541): cached reciprocal with one FMA correction
+    __device__ static double quotient(double delta, double direction, double inverse)
+    {
+        if (inverse == 0.0) return delta / direction;
+        const double q = delta * inverse;
+        if (!isfinite(q) || fabs(q) < 2.2250738585072014e-308) return delta / direction;
+        return fma(fma(-q, direction, delta), inverse, q);
+    }
+    __device__ double crossing(const Ray64& r, int axis, const int* shape, double upper) const
+    {
+        if (r.direction[axis] == 0.0 || plane[axis] < 0 || plane[axis] >= shape[axis]) return upper;
+        const double c = quotient((double)plane[axis] - r.origin[axis], r.direction[axis], inverse[axis]);
+        return c < upper ? c : upper;
+    }
+    // reference begin_cells (:559-611)
+    __device__ void begin(const Ray64& r, double lower, double upper, const int* shape)
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double entry = fma(lower, r.direction[a], r.origin[a]);
+            const double v = r.direction[a];
+            inverse[a] = 0.0;
+            step[a] = 0;
+            plane[a] = 0;
+            if (v != 0.0) {
+                const double inv = 1.0 / v;
+                if (isfinite(inv) && fabs(inv) >= 2.2250738585072014e-308 && fabs(v) >= 2.2250738585072014e-308)
+                    inverse[a] = inv;
+            }
+            if (v > 0.0) {
+                step[a] = 1;
+                const int c = (int)ceil(entry);
+                plane[a] = c > 0 ? c : 0;
+            } else if (v < 0.0) {
+                step[a] = -1;
+                const int c = (int)floor(entry);
+                plane[a] = c < shape[a] - 1 ? c : shape[a] - 1;
+            }
+            double c = crossing(r, a, shape, upper);
+            if (c <= lower) {
+                plane[a] += step[a];
+                c = crossing(r, a, shape, upper);
+            }
+            next[a] = c;
+        }
+    }
+    // reference cell_segment (:614-646)
+    __device__ void segment(const Ray64& r, double start, const FieldDims& d, GaussSegment& s) const
+    {
+        const double n12 = next[1] < next[2] ? next[1] : next[2];
+        s.end = next[0] < n12 ? next[0] : n12;
+        s.radius = (s.end - start) * 0.5;
+        const double centre = start + s.radius;
+        const double offset = s.radius / sqrt(3.0);
+        s.first_position = centre - offset;
+        s.second_position = centre + offset;
+        double mid[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            s.first[a] = fma(s.first_position, r.direction[a], r.origin[a]);
+            s.second[a] = fma(s.second_position, r.direction[a], r.origin[a]);
+            mid[a] = fma(centre, r.direction[a], r.origin[a]);
+        }
+        const int shape[3] = {d.nx, d.ny, d.nz}, cap[3] = {d.cx, d.cy, d.cz};
+        s.shared = true;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double high = (double)(shape[a] - 1);
+            s.lower[a] = axis64(mid[a], high, cap[a]).lower;
+            const double low = (double)s.lower[a], up = low + 1.0;
+            const double c1 = fmin(fmax(s.first[a], 0.0), high), c2 = fmin(fmax(s.second[a], 0.0), high);
+            if (c1 < low || c2 < low) s.shared = false;
+            if (s.lower[a] < shape[a] - 2 && (c1 >= up || c2 >= up)) s.shared = false;
+        }
+    }
+    // reference advance_cells (:649-660)
+    __device__ void advance(const Ray64& r, const int* shape, double end, double upper)
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (next[a] <= end) {
+                plane[a] += step[a];
+                next[a] = crossing(r, a, shape, upper);
+            }
+        }
+    }
+};
+
 // Compensated ray sum of the precision form: 16-sample blocks summed serially in FP32,
 // block sums added with Kahan compensation.  Blocks are aligned to the sample index.
 struct BlockSum {

@@ -58,6 +58,8 @@ extern "C" int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_ray
         return DPT_E_NULL;
     if (problem->field_dtype != DPT_F32) return DPT_E_DTYPE;
     if (components != 12 && components != 6) return DPT_E_FLAGS;
+    // the mixed and fast samplings are fixed-pose forms
+    if (problem->arith == DPT_ARITH_MIXED || problem->arith == DPT_ARITH_FAST) return DPT_E_FLAGS;
     dpt_problem direct = *problem;
     direct.layout = DPT_LAYOUT_DIRECT;  // sample the caller's field: no replicated copy
     // the size query returns 0 for every problem the other entry points reject

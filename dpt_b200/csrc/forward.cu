@@ -147,6 +147,134 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
             if (!isfinite(total)) bits |= 2;
             result = total;
         }
+    } else if constexpr (kArith == DPT_ARITH_CELLS) {
+        // reference integration="cell_gauss" (kernels/projection.py:717-746, segment action
+        // :695-711): two Gauss nodes per cell segment, L = length * sum radius * value
+        if (!valid_ray(r)) {
+            bits = 2;
+        } else {
+            Interval<double> iv;
+            iv.clip(r.origin, r.direction, a.grid.nx, a.grid.ny, a.grid.nz);
+            double integral = 0.0;
+            if (iv.upper > iv.lower) {
+                FieldDims dims;
+                dims.init(a.grid);
+                const int shape[3] = {dims.nx, dims.ny, dims.nz};
+                CellWalk64 walk;
+                walk.begin(r, iv.lower, iv.upper, shape);
+                double start = iv.lower;
+                const int64_t limit = (int64_t)shape[0] + shape[1] + shape[2] + 1;
+                for (int64_t segments = 0; start < iv.upper && segments < limit; ++segments) {
+                    GaussSegment s;
+                    walk.segment(r, start, dims, s);
+                    if (s.end <= start) {
+                        bits |= 2;
+                        break;
+                    }
+                    if (!finite3(s.first[0], s.first[1], s.first[2]) ||
+                        !finite3(s.second[0], s.second[1], s.second[2]))
+                        bits |= 2;
+                    integral = fma(s.radius, sample_strict64(f, dims, s.first, nullptr), integral);
+                    integral = fma(s.radius, sample_strict64(f, dims, s.second, nullptr), integral);
+                    start = s.end;
+                    walk.advance(r, shape, s.end, iv.upper);
+                }
+                if (start < iv.upper) bits |= 2;
+                integral = integral * r.length;
+            }
+            result = integral;
+            if (!finite_out<Out>(result)) bits |= 2;
+        }
+    } else if constexpr (kArith == DPT_ARITH_MIXED || kArith == DPT_ARITH_FAST) {
+        // reference mixed_float32 / fast_float32 (kernels/projection.py:296-392): FP64 clip,
+        // FP32 marching and clamped corner weights, the corner sum in FP64 (MIXED) or as an
+        // FP32 fmaf chain promoted to the FP64 ray sum (FAST)
+        if (!valid_ray(r)) {
+            bits = 2;
+        } else {
+            Interval<double> iv;
+            iv.clip(r.origin, r.direction, a.grid.nx, a.grid.ny, a.grid.nz);
+            double integral = 0.0;
+            if (iv.upper > iv.lower) {
+                FieldDims dims;
+                dims.init(a.grid);
+                const double step = (iv.upper - iv.lower) / (double)S;
+                float entry[3], sv[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
+                    sv[k] = (float)(step * r.direction[k]);
+                }
+                auto at = [&](int i, float& x, float& y, float& z) {
+                    const float offset = (float)i + 0.5f;
+                    x = fmaf(offset, sv[0], entry[0]);
+                    y = fmaf(offset, sv[1], entry[1]);
+                    z = fmaf(offset, sv[2], entry[2]);
+                };
+                CellCache<Field> cache;
+                auto add = [&](Axis32 X, Axis32 Y, Axis32 Z) {
+                    cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
+                    float w[8];
+                    corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+                    if constexpr (kArith == DPT_ARITH_FAST) {
+                        float value = 0.0f;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) value = fmaf(w[c], cache.v[c], value);
+                        integral = integral + (double)value;
+                    } else {
+                        double value = 0.0;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) value = fma((double)w[c], (double)cache.v[c], value);
+                        integral = integral + value;
+                    }
+                };
+                auto sample = [&](int i) {
+                    float x, y, z;
+                    at(i, x, y, z);
+                    if (inside(x, y, z, dims.hx, dims.hy, dims.hz))
+                        add(axis32(x, dims.mx, dims.cx), axis32(y, dims.my, dims.cy), axis32(z, dims.mz, dims.cz));
+                    else
+                        integral = integral + 0.0;
+                };
+                if (!moderate(entry, sv)) {
+                    bool finite = true;
+                    for (int i = 0; i < S; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        finite = finite && finite3f(x, y, z);
+                        sample(i);
+                    }
+                    if (!finite) bits |= 2;
+                } else {
+                    int first, last;
+                    inside_run(S, [&](int i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        return inside(x, y, z, dims.hx, dims.hy, dims.hz);
+                    }, first, last);
+                    int ifirst, ilast;
+                    interior_run(first, last, [&](int i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
+                    }, ifirst, ilast);
+                    const int split = min(ifirst, last + 1);
+                    for (int i = first; i < split; ++i) sample(i);
+#pragma unroll 2
+                    for (int i = ifirst; i <= ilast; ++i) {
+                        float x, y, z;
+                        at(i, x, y, z);
+                        add(interior_axis(x), interior_axis(y), interior_axis(z));
+                    }
+                    for (int i = max(ilast + 1, split); i <= last; ++i) sample(i);
+                    // the zero samples after the run: adding +0 only turns -0 into +0
+                    if (last < S - 1) integral = integral + 0.0;
+                }
+                integral = integral * (r.length * step);
+            }
+            result = integral;
+            if (!finite_out<Out>(result)) bits |= 2;
+        }
     } else if constexpr (kArith == DPT_ARITH_F64) {
         if (!valid_ray(r)) {
             bits = 2;
@@ -365,16 +493,20 @@ cudaError_t launch_forward(const dpt_problem& p, const RayArgs& a, const void* p
         PolyF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
         return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
     }
-    // FP32 storage only from here (half storage is compensated and replicated, handled above)
-    if (p.layout == DPT_LAYOUT_DIRECT) {
-        PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
-        if (p.arith == DPT_ARITH_F32) return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
-        if (p.arith == DPT_ARITH_F64) return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
-        return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
-    }
-    QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
-    if (p.arith == DPT_ARITH_F32) return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
-    return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
+    // direct gathers from the caller's FP32 field, or the FP32 corner quads (decoded from any
+    // storage type by the pack kernel)
+    auto run = [&](const auto& f) -> cudaError_t {
+        switch (p.arith) {
+        case DPT_ARITH_F32: return forward_with<DPT_ARITH_F32>(p, a, f, image, grid, stream);
+        case DPT_ARITH_F64: return forward_with<DPT_ARITH_F64>(p, a, f, image, grid, stream);
+        case DPT_ARITH_MIXED: return forward_with<DPT_ARITH_MIXED>(p, a, f, image, grid, stream);
+        case DPT_ARITH_FAST: return forward_with<DPT_ARITH_FAST>(p, a, f, image, grid, stream);
+        case DPT_ARITH_CELLS: return forward_with<DPT_ARITH_CELLS>(p, a, f, image, grid, stream);
+        default: return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
+        }
+    };
+    if (p.layout == DPT_LAYOUT_DIRECT) return run(PlainF32{static_cast<const float*>(packed), p.nx, p.ny, p.nz});
+    return run(QuadF32{static_cast<const float4*>(packed), p.nx, p.ny, p.nz});
 }
 
 cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower, double* upper,
@@ -383,9 +515,9 @@ cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower,
     const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
     if (p.arith == DPT_ARITH_F32)
         k_counts<DPT_ARITH_F32><<<grid, kBlock, 0, stream>>>(a, lower, upper, realised);
-    else if (p.arith == DPT_ARITH_F64)
+    else if (p.arith == DPT_ARITH_F64 || p.arith == DPT_ARITH_CELLS)
         k_counts<DPT_ARITH_F64><<<grid, kBlock, 0, stream>>>(a, lower, upper, realised);
-    else
+    else  // F32C, MIXED and FAST share the FP64 clip and the FP32 marching
         k_counts<DPT_ARITH_F32C><<<grid, kBlock, 0, stream>>>(a, lower, upper, realised);
     return cudaGetLastError();
 }

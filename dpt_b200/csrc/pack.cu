@@ -40,6 +40,7 @@ __device__ bool rigid_pose(const double* p)
 
 struct PackArgs {
     int nx, ny, nz;
+    int signed_domain;  // DPT_DOMAIN_SIGNED: only non-finite values are flagged
     int64_t voxels;
     int views;
     const double* poses;
@@ -61,7 +62,22 @@ __device__ __forceinline__ void check_pose(const PackArgs& a, int64_t index)
     }
 }
 
-__global__ void __launch_bounds__(256) k_pack_quad(PackArgs a, const float* __restrict__ field,
+template <int kDtype>
+__device__ __forceinline__ float decode(const void* field, int64_t index)
+{
+    if constexpr (kDtype == DPT_F32) return static_cast<const float*>(field)[index];
+    else if constexpr (kDtype == DPT_BF16) return bf16_bits_to_float(static_cast<const uint16_t*>(field)[index]);
+    else return half_bits_to_float(static_cast<const uint16_t*>(field)[index]);
+}
+
+__device__ __forceinline__ bool out_of_domain(const PackArgs& a, float v)
+{
+    return !isfinite(v) || (!a.signed_domain && v < 0.0f);
+}
+
+// FP32 corner quads of any storage type (half values decoded exactly).
+template <int kDtype>
+__global__ void __launch_bounds__(256) k_pack_quad(PackArgs a, const void* __restrict__ field,
                                                    float4* __restrict__ quad)
 {
     const int64_t index = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -72,21 +88,16 @@ __global__ void __launch_bounds__(256) k_pack_quad(PackArgs a, const float* __re
     const int y = (int)(rest % a.ny), z = (int)(rest / a.ny);
     const int x1 = min(x + 1, a.nx - 1), y1 = min(y + 1, a.ny - 1);
     const int64_t row0 = ((int64_t)z * a.ny + y) * a.nx, row1 = ((int64_t)z * a.ny + y1) * a.nx;
-    const float v = field[index];
-    flag_field(!isfinite(v) || v < 0.0f, a.status);
-    if (quad) quad[index] = make_float4(v, field[row0 + x1], field[row1 + x], field[row1 + x1]);
+    const float v = decode<kDtype>(field, index);
+    flag_field(out_of_domain(a, v), a.status);
+    if (quad)
+        quad[index] = make_float4(v, decode<kDtype>(field, row0 + x1), decode<kDtype>(field, row1 + x),
+                                  decode<kDtype>(field, row1 + x1));
 }
 
 // Polynomial copy of the compensated precision form: per cell the coefficients of
 // f = c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz from its eight decoded corner
 // values (clamped like corner_index), in the order and FP32 arithmetic of PolyCache.
-template <int kDtype>
-__device__ __forceinline__ float decode(const void* field, int64_t index)
-{
-    if constexpr (kDtype == DPT_F32) return static_cast<const float*>(field)[index];
-    else if constexpr (kDtype == DPT_BF16) return bf16_bits_to_float(static_cast<const uint16_t*>(field)[index]);
-    else return half_bits_to_float(static_cast<const uint16_t*>(field)[index]);
-}
 
 template <int kDtype>
 __global__ void __launch_bounds__(256) k_pack_poly(PackArgs a, const void* __restrict__ field,
@@ -99,7 +110,7 @@ __global__ void __launch_bounds__(256) k_pack_poly(PackArgs a, const void* __res
     const int64_t rest = index / a.nx;
     const int y = (int)(rest % a.ny), z = (int)(rest / a.ny);
     const float own = decode<kDtype>(field, index);
-    flag_field(!isfinite(own) || own < 0.0f, a.status);
+    flag_field(out_of_domain(a, own), a.status);
     if (!coef) return;  // validation only
     const int x1 = min(x + 1, a.nx - 1), y1 = min(y + 1, a.ny - 1), z1 = min(z + 1, a.nz - 1);
     const int64_t r00 = ((int64_t)z * a.ny + y) * a.nx, r10 = ((int64_t)z * a.ny + y1) * a.nx;
@@ -130,6 +141,7 @@ cudaError_t launch_prepare_field(const dpt_problem& p, const void* field, void* 
     a.ny = p.ny;
     a.nz = p.nz;
     a.voxels = (int64_t)p.nx * p.ny * p.nz;
+    a.signed_domain = p.field_domain == DPT_DOMAIN_SIGNED;
     a.views = p.views;
     a.poses = poses;
     a.status = status;
@@ -144,8 +156,13 @@ cudaError_t launch_prepare_field(const dpt_problem& p, const void* field, void* 
         else
             k_pack_poly<DPT_F16><<<blocks, 256, 0, stream>>>(a, field, coef);
     } else {
-        k_pack_quad<<<blocks, 256, 0, stream>>>(a, static_cast<const float*>(field),
-                                                static_cast<float4*>(packed));
+        float4* quad = static_cast<float4*>(packed);
+        if (p.field_dtype == DPT_F32)
+            k_pack_quad<DPT_F32><<<blocks, 256, 0, stream>>>(a, field, quad);
+        else if (p.field_dtype == DPT_BF16)
+            k_pack_quad<DPT_BF16><<<blocks, 256, 0, stream>>>(a, field, quad);
+        else
+            k_pack_quad<DPT_F16><<<blocks, 256, 0, stream>>>(a, field, quad);
     }
     return cudaGetLastError();
 }

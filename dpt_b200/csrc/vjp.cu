@@ -308,6 +308,208 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
                     }
                 }
             }
+        } else if constexpr (kArith == DPT_ARITH_MIXED || kArith == DPT_ARITH_FAST) {
+            // reference mixed / fast sampling, fixed pose (kernels/projection.py:1026-1106 with
+            // the mixed scatter :431-479): each inside sample adds, per corner, the FP32
+            // rounding of volume_factor * w_c, w_c the forward's FP32 corner weight
+            if (!valid_ray(r)) {
+                bits = 2;
+            } else if (kVol) {
+                Interval<double> iv;
+                iv.clip(r.origin, r.direction, dims.nx, dims.ny, dims.nz);
+                double span = iv.upper - iv.lower;
+                const double seed = seed_in;
+                if (!isfinite(seed)) bits |= 2;
+                if (seed == 0.0) span = 0.0;
+                if (span > 0.0) {
+                    const double vf = seed * r.length * span / (double)S;
+                    const double step = span / (double)S;
+                    float entry[3], sv[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        entry[k] = (float)fma(iv.lower, r.direction[k], r.origin[k]);
+                        sv[k] = (float)(step * r.direction[k]);
+                    }
+                    float cs[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                    int pending = -1;
+                    auto flush = [&]() {
+                        flush_cell(acc, pending, cs);
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                    };
+                    auto visit = [&](int i, bool general) {
+                        const float offset = (float)i + 0.5f;
+                        const float x = fmaf(offset, sv[0], entry[0]);
+                        const float y = fmaf(offset, sv[1], entry[1]);
+                        const float z = fmaf(offset, sv[2], entry[2]);
+                        if (general) {
+                            if (!finite3f(x, y, z)) bits |= 2;
+                            if (!inside(x, y, z, dims.hx, dims.hy, dims.hz)) {
+                                if (pending >= 0) flush();
+                                pending = -1;
+                                return;
+                            }
+                        }
+                        const Axis32 X = axis32(x, dims.mx, dims.cx), Y = axis32(y, dims.my, dims.cy),
+                                     Z = axis32(z, dims.mz, dims.cz);
+                        const int cell = (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower;
+                        if (cell != pending) {
+                            if (pending >= 0) flush();
+                            pending = cell;
+                        }
+                        float w[8];
+                        corner_weights(X.fraction, Y.fraction, Z.fraction, w);
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            const float increment = (float)(vf * (double)w[c]);
+                            if (!isfinite(increment)) bits |= 2;
+                            cs[c] = cs[c] + increment;
+                        }
+                    };
+                    if (!moderate(entry, sv)) {
+                        for (int i = 0; i < S; ++i) visit(i, true);
+                    } else {
+                        int first, last;
+                        inside_run(S, [&](int i) {
+                            const float offset = (float)i + 0.5f;
+                            return inside(fmaf(offset, sv[0], entry[0]), fmaf(offset, sv[1], entry[1]),
+                                          fmaf(offset, sv[2], entry[2]), dims.hx, dims.hy, dims.hz);
+                        }, first, last);
+                        for (int i = first; i <= last; ++i) visit(i, false);
+                    }
+                    if (pending >= 0) flush();
+                }
+            }
+        } else if constexpr (kArith == DPT_ARITH_CELLS) {
+            // reference cell-Gauss VJP (kernels/projection.py:935-1024 and the shared tail
+            // 1152-1210): Gauss-node gradients weighted by radius (origin) and radius times
+            // position (direction), the zero-extended support's endpoint terms, factor =
+            // seed * length; the scatter combines a shared cell's two nodes before rounding
+            if (!valid_ray(r)) {
+                bits = 2;
+            } else {
+                Interval<double> iv;
+                iv.clip(r.origin, r.direction, dims.nx, dims.ny, dims.nz);
+                double span = iv.upper - iv.lower;
+                const double seed = seed_in;
+                if (!isfinite(seed)) bits |= 2;
+                if (seed == 0.0) span = 0.0;
+                if (span > 0.0) {
+                    const double factor = seed * r.length;
+                    const int shape[3] = {dims.nx, dims.ny, dims.nz}, cap[3] = {dims.cx, dims.cy, dims.cz};
+                    double og[3] = {0.0, 0.0, 0.0}, dg[3] = {0.0, 0.0, 0.0};
+                    // one node's FP64 corner terms ((seed w0) w1) w2 relative to cell `lower`
+                    auto corner_terms = [&](const double* q, const int* lower, double vf, double* t) {
+                        double fr[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            fr[k] = fmin(fmax(q[k], 0.0), (double)(shape[k] - 1)) - (double)lower[k];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            double contribution = vf * ((c & 1) ? fr[0] : 1.0 - fr[0]);
+                            contribution = contribution * ((c & 2) ? fr[1] : 1.0 - fr[1]);
+                            t[c] = contribution * ((c & 4) ? fr[2] : 1.0 - fr[2]);
+                        }
+                    };
+                    auto scatter_node = [&](const double* q, double vf) {
+                        if (!inside(q[0], q[1], q[2], dims.nx, dims.ny, dims.nz)) return;
+                        int lower[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) lower[k] = axis64(q[k], (double)(shape[k] - 1), cap[k]).lower;
+                        double t[8];
+                        corner_terms(q, lower, vf, t);
+                        float c32[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            c32[c] = (float)t[c];
+                            if (!isfinite(c32[c])) bits |= 2;
+                        }
+                        flush_cell(acc, (lower[2] * dims.ny + lower[1]) * dims.nx + lower[0], c32);
+                    };
+                    CellWalk64 walk;
+                    walk.begin(r, iv.lower, iv.upper, shape);
+                    double start = iv.lower;
+                    const int64_t limit = (int64_t)shape[0] + shape[1] + shape[2] + 1;
+                    for (int64_t segments = 0; start < iv.upper && segments < limit; ++segments) {
+                        GaussSegment s;
+                        walk.segment(r, start, dims, s);
+                        if (s.end <= start) {
+                            bits |= 2;
+                            break;
+                        }
+                        if (!finite3(s.first[0], s.first[1], s.first[2]) ||
+                            !finite3(s.second[0], s.second[1], s.second[2]))
+                            bits |= 2;
+                        if (kPose) {
+                            double g1[3], g2[3];
+                            sample_strict64(f, dims, s.first, g1);
+                            sample_strict64(f, dims, s.second, g2);
+                            const double r1 = s.radius * s.first_position, r2 = s.radius * s.second_position;
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                og[k] = fma(s.radius, g1[k], og[k]);
+                                og[k] = fma(s.radius, g2[k], og[k]);
+                                dg[k] = fma(r1, g1[k], dg[k]);
+                                dg[k] = fma(r2, g2[k], dg[k]);
+                            }
+                        }
+                        if (kVol) {
+                            const double vf = factor * s.radius;
+                            if (s.shared) {
+                                const bool in1 = inside(s.first[0], s.first[1], s.first[2], dims.nx, dims.ny, dims.nz);
+                                const bool in2 = inside(s.second[0], s.second[1], s.second[2], dims.nx, dims.ny, dims.nz);
+                                double t1[8], t2[8];
+                                corner_terms(s.first, s.lower, in1 ? vf : 0.0, t1);
+                                corner_terms(s.second, s.lower, in2 ? vf : 0.0, t2);
+                                float c32[8];
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) {
+                                    c32[c] = (float)(t1[c] + t2[c]);
+                                    if (!isfinite(c32[c])) bits |= 2;
+                                }
+                                flush_cell(acc, (s.lower[2] * dims.ny + s.lower[1]) * dims.nx + s.lower[0], c32);
+                            } else {
+                                scatter_node(s.first, vf);
+                                scatter_node(s.second, vf);
+                            }
+                        }
+                        start = s.end;
+                        walk.advance(r, shape, s.end, iv.upper);
+                    }
+                    if (start < iv.upper) bits |= 2;
+                    if (kPose) {
+                        double lower_point[3], upper_point[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            // support_value (:663-674): the endpoint clamped into the support
+                            const double high = (double)shape[k] - 0.5;
+                            lower_point[k] = fmin(fmax(fma(iv.lower, r.direction[k], r.origin[k]), -0.5), high);
+                            upper_point[k] = fmin(fmax(fma(iv.upper, r.direction[k], r.origin[k]), -0.5), high);
+                        }
+                        const double lower_value = sample_strict64(f, dims, lower_point, nullptr);
+                        const double upper_value = sample_strict64(f, dims, upper_point, nullptr);
+                        double lo_o[3], lo_d[3], up_o[3], up_d[3];
+                        iv.lower_gradients(lo_o, lo_d);
+                        iv.upper_gradients(up_o, up_d);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            og[k] = og[k] + fma(-lower_value, lo_o[k], upper_value * up_o[k]);
+                            dg[k] = dg[k] + fma(-lower_value, lo_d[k], upper_value * up_d[k]);
+                        }
+                        double sa[3], da[3];
+                        matvec_t(a.grid.m, og, sa);
+                        matvec_t(a.grid.m, dg, da);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            sa[k] = factor * sa[k];
+                            da[k] = factor * da[k];
+                        }
+                        pose_epilogue(a, vs, view, pixel, mode, sa, da, g);
+                    }
+                }
+            }
         } else if constexpr (kArith == DPT_ARITH_F64) {
             if (!valid_ray(r)) {
                 bits = 2;
@@ -708,12 +910,18 @@ cudaError_t vjp_with(const RayArgs& a, const Field& f, const Seed* cot, int flag
     const bool volume = (flags & DPT_VJP_VOLUME) != 0;
     const bool pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
     const int mode = (flags & DPT_VJP_POSE12) ? 12 : ((flags & DPT_VJP_PER_RAY6) ? -6 : 6);
-    if (volume && pose)
-        k_vjp<kArith, Field, true, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
-    else if (volume)
+    if constexpr (kArith == DPT_ARITH_MIXED || kArith == DPT_ARITH_FAST) {
+        // fixed-pose forms: the C ABI admits the volume cotangent only
+        if (pose || !volume) return cudaErrorInvalidValue;
         k_vjp<kArith, Field, true, false, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
-    else
-        k_vjp<kArith, Field, false, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+    } else {
+        if (volume && pose)
+            k_vjp<kArith, Field, true, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+        else if (volume)
+            k_vjp<kArith, Field, true, false, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+        else
+            k_vjp<kArith, Field, false, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+    }
     return cudaGetLastError();
 }
 
@@ -736,19 +944,26 @@ cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packe
         PolyF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
         return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
     }
-    // FP32 storage only from here (half storage is compensated and replicated, handled above)
-    if (p.layout == DPT_LAYOUT_DIRECT) {
-        PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
-        if (p.arith == DPT_ARITH_F32)
+    // direct gathers from the caller's FP32 field, or the FP32 corner quads (decoded from any
+    // storage type by the pack kernel)
+    auto run = [&](const auto& f) -> cudaError_t {
+        switch (p.arith) {
+        case DPT_ARITH_F32:
             return vjp_seed<DPT_ARITH_F32>(p, a, f, cotangent, flags, accumulator, partials, stream);
-        if (p.arith == DPT_ARITH_F64)
+        case DPT_ARITH_F64:
             return vjp_seed<DPT_ARITH_F64>(p, a, f, cotangent, flags, accumulator, partials, stream);
-        return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
-    }
-    QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
-    if (p.arith == DPT_ARITH_F32)
-        return vjp_seed<DPT_ARITH_F32>(p, a, f, cotangent, flags, accumulator, partials, stream);
-    return vjp_seed<DPT_ARITH_F64>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        case DPT_ARITH_MIXED:
+            return vjp_seed<DPT_ARITH_MIXED>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        case DPT_ARITH_FAST:
+            return vjp_seed<DPT_ARITH_FAST>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        case DPT_ARITH_CELLS:
+            return vjp_seed<DPT_ARITH_CELLS>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        default:
+            return vjp_seed<DPT_ARITH_F32C>(p, a, f, cotangent, flags, accumulator, partials, stream);
+        }
+    };
+    if (p.layout == DPT_LAYOUT_DIRECT) return run(PlainF32{static_cast<const float*>(packed), p.nx, p.ny, p.nz});
+    return run(QuadF32{static_cast<const float4*>(packed), p.nx, p.ny, p.nz});
 }
 
 }  // namespace dpt

@@ -116,6 +116,7 @@ class RayPlan:
         image_dtype: int = N.F32,
         layout: int = N.LAYOUT_REPLICATED,
         block_cols: int = 0,
+        field_domain: int = N.DOMAIN_PHYSICAL,
     ) -> N.Problem:
         nz, ny, nx = self.grid.shape
         p = N.Problem()
@@ -128,6 +129,7 @@ class RayPlan:
         p.image_dtype = image_dtype
         p.layout = layout
         p.block_cols = block_cols
+        p.field_domain = field_domain
         for k in range(9):
             p.object_to_grid[k] = self.object_to_grid[k]
         for k in range(3):

@@ -37,29 +37,39 @@ from .contracts import ContractError, NumericalError, integer, raise_device_stat
 from .plan import RayPlan, plan_rays
 from .volumes import GridSpec
 
-SamplingPrecision = Literal["float32", "float64", "compensated"]
+SamplingPrecision = Literal["float32", "float64", "mixed_float32", "fast_float32", "compensated"]
 StoragePrecision = Literal["float32", "float16", "bfloat16"]
 
 _STORAGE = {"float32": (N.F32, torch.float32), "float16": (N.F16, torch.float16),
             "bfloat16": (N.BF16, torch.bfloat16)}
-_ARITH = {"float32": N.ARITH_F32, "float64": N.ARITH_F64, "compensated": N.ARITH_F32C}
+_ARITH = {"float32": N.ARITH_F32, "float64": N.ARITH_F64, "mixed_float32": N.ARITH_MIXED,
+          "fast_float32": N.ARITH_FAST, "compensated": N.ARITH_F32C}
 
 
 @dataclass(frozen=True, slots=True)
 class ProjectionSpec:
-    """Quadrature and arithmetic of one projector.
+    """Quadrature and arithmetic of one projector (reference ``ProjectionSpec``,
+    python/dpt/projection.py:67-140, with this build's launch options).
 
-    ``samples_per_ray`` midpoints per clipped ray.  ``sampling_precision``:
-    ``"float32"`` is the reference FP32 projector (FP64 ray setup, FP32 clip,
-    interpolation and serial ray sum), ``"float64"`` the reference strict FP64
-    projector, ``"compensated"`` FP64 setup and clip with FP32 marching,
-    interpolation and a compensated (Kahan) ray sum - the form used for FP16 and
-    BF16 storage.  ``precision`` is the image / cotangent dtype.
-    ``widen_views`` is how many views accumulate in FP32 before the volume
-    gradient is widened into its FP64 total (the reference uses 8 for FP32 and 2
-    for FP64 sampling).  ``layout`` selects the corner-replicated field copy or
-    direct gathers; ``block_cols`` the detector tile of one 256-ray block (8, 16,
-    32 or 64 columns; 0 = 16), a launch-shape choice that does not change results.
+    ``integration``: ``"midpoint"`` uses ``samples_per_ray`` clipped midpoints;
+    ``"cell_gauss"`` splits the ray at every interpolation plane and integrates each
+    cubic segment exactly with two Gauss nodes (FP64 sampling; the sample count is then
+    ignored).  ``sampling_precision``: ``"float64"`` the reference strict projector;
+    ``"float32"`` the reference FP32 projector (FP64 ray setup, FP32 clip, interpolation
+    and serial ray sum; FP32 storage); ``"mixed_float32"`` FP32 marching and corner
+    weights with FP64 products and sums, ``"fast_float32"`` the same with an FP32 cell
+    sum (both fixed-pose); ``"compensated"`` this build's precision form for FP16/BF16
+    storage (closed-form sums over the cell runs, compensated FP32 ray sum).
+    ``storage_precision`` FP32, FP16 or BF16 field storage (decoded exactly on the
+    device); ``field_domain`` ``"physical"`` (finite, non-negative attenuation) or
+    ``"signed_linear"`` (any finite value); ``validate`` ``"once"``/``"always"`` check
+    field and poses on every call (the check is fused into the pass that writes the
+    field copy), ``"never"`` skips reading the status words back.  ``precision`` is the
+    image / cotangent dtype.  ``widen_views`` is how many views accumulate in FP32
+    before the volume gradient is widened into its FP64 total (the reference uses 8 for
+    FP32 and 2 for FP64 sampling).  ``layout`` selects the field copy or direct gathers;
+    ``block_cols`` the detector tile of one block (8, 16, 32 or 64 columns; 0 = 16), a
+    launch-shape choice that does not change results.
     """
 
     samples_per_ray: int
@@ -71,19 +81,37 @@ class ProjectionSpec:
     widen_views: int | None = None
     layout: Literal["replicated", "direct"] = "replicated"
     block_cols: int = 0
+    integration: Literal["midpoint", "cell_gauss"] = "midpoint"
+    field_domain: Literal["physical", "signed_linear"] = "physical"
+    validate: Literal["once", "always", "never"] = "once"
 
     def __post_init__(self) -> None:
         integer(self.samples_per_ray, "samples_per_ray", minimum=1)
+        if self.integration not in ("midpoint", "cell_gauss"):
+            raise ContractError("projection integration must be midpoint or cell_gauss")
         if self.precision not in ("float32", "float64"):
             raise ContractError("projection precision must be float32 or float64")
+        if self.field_domain not in ("physical", "signed_linear"):
+            raise ContractError("projection field_domain must be physical or signed_linear")
         if self.sampling_precision not in _ARITH:
-            raise ContractError("sampling_precision must be float32, float64 or compensated")
+            raise ContractError("sampling_precision must be float32, float64, mixed_float32, fast_float32 "
+                                "or compensated")
         if self.storage_precision not in _STORAGE:
             raise ContractError("storage_precision must be float32, float16 or bfloat16")
-        if self.storage_precision != "float32" and self.sampling_precision != "compensated":
-            raise ContractError("FP16/BF16 storage requires compensated FP32 sampling")
+        if self.sampling_precision in ("mixed_float32", "fast_float32") and (
+            self.integration != "midpoint" or self.active_pose
+        ):
+            raise ContractError("FP32 sampling requires midpoint integration and fixed pose")
+        if self.sampling_precision == "float32" and (
+            self.integration != "midpoint" or self.storage_precision != "float32"
+        ):
+            raise ContractError("FP32 arithmetic requires midpoint integration and FP32 field storage")
+        if self.sampling_precision == "compensated" and self.integration != "midpoint":
+            raise ContractError("compensated sampling requires midpoint integration")
         if type(self.active_pose) is not bool or type(self.active_volume) is not bool:
             raise ContractError("active input flags must be booleans")
+        if self.validate not in ("once", "always", "never"):
+            raise ContractError("projection validate must be once, always or never")
         if self.widen_views is not None:
             integer(self.widen_views, "widen_views", minimum=1)
         if self.layout not in ("replicated", "direct"):
@@ -95,7 +123,13 @@ class ProjectionSpec:
 
     @property
     def arith(self) -> int:
+        if self.integration == "cell_gauss":
+            return N.ARITH_CELLS
         return _ARITH[self.sampling_precision]
+
+    @property
+    def domain_code(self) -> int:
+        return N.DOMAIN_SIGNED if self.field_domain == "signed_linear" else N.DOMAIN_PHYSICAL
 
     @property
     def field_code(self) -> int:
@@ -117,7 +151,7 @@ class ProjectionSpec:
     def batch_views(self) -> int:
         if self.widen_views is not None:
             return self.widen_views
-        return 2 if self.sampling_precision == "float64" else 8
+        return 2 if self.sampling_precision in ("float64", "mixed_float32", "fast_float32") else 8
 
 
 def _ptr(tensor: torch.Tensor | None) -> int | None:
@@ -220,6 +254,7 @@ class ProjectionWorkspace:
             image_dtype=spec.image_code,
             layout=N.LAYOUT_DIRECT if spec.layout == "direct" else N.LAYOUT_REPLICATED,
             block_cols=spec.block_cols,
+            field_domain=spec.domain_code,
         )
         with torch.cuda.device(device):
             self.view_table = (
@@ -414,7 +449,7 @@ class ProjectionWorkspace:
             self._run("forward", lambda: N.library().dpt_b200_forward(self.problem, self.rays(poses), packed.data_ptr(),
                                              out.data_ptr(), self.status.data_ptr(),
                                              _stream(self.device)))
-            if checked:
+            if checked and self.spec.validate != "never":
                 self.consume_status()
             return out
 
@@ -475,7 +510,7 @@ class ProjectionWorkspace:
                 self._run("finish_pose", lambda: lib.dpt_b200_finish_pose(self.problem, 0, self.views, components,
                                              partials.data_ptr(), pose_gradient.data_ptr(), 0,
                                              self.status.data_ptr(), stream))
-            if checked:
+            if checked and self.spec.validate != "never":
                 self.consume_status()
             return gradient, pose_gradient
 
@@ -491,7 +526,7 @@ class ProjectionWorkspace:
             self._run("pose_sensitivities", lambda: N.library().dpt_b200_vjp(self.problem, self.rays(poses), packed.data_ptr(),
                                          cot.data_ptr(), N.VJP_PER_RAY6, None, out.data_ptr(),
                                          self.status.data_ptr(), _stream(self.device)))
-            if checked:
+            if checked and self.spec.validate != "never":
                 self.consume_status()
             return out
 

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define DPT_B200_ABI_VERSION 1
+#define DPT_B200_ABI_VERSION 2
 
 /* Storage / output element types. */
 enum {
@@ -61,12 +61,31 @@ enum {
  *                  (the reference "fp32" Projector, kernels/projection_fp32.py).
  *  DPT_ARITH_F64   FP64 ray setup, clip, interpolation and sum (the reference "fp64" Projector,
  *                  kernels/projection.py strict midpoint).
- *  DPT_ARITH_F32C  FP64 ray setup and clip, FP32 marching and interpolation, compensated
- *                  (Kahan) FP32 ray sum; the precision form for FP16/BF16 (and FP32) storage. */
+ *  DPT_ARITH_F32C  FP64 ray setup and clip, FP32 marching, closed-form sums over the cell runs
+ *                  of each ray, compensated FP32 sum over runs; the precision form for
+ *                  FP16/BF16 (and FP32) storage (no reference counterpart).
+ *  DPT_ARITH_MIXED FP64 setup and clip, FP32 marching and corner weights, FP64 products and
+ *                  ray sum (the reference "mixed_float32" sampling, kernels/projection.py:296-392);
+ *                  fixed pose: the VJP takes DPT_VJP_VOLUME only.
+ *  DPT_ARITH_FAST  as MIXED with an FP32 fmaf cell sum promoted to the FP64 ray sum (the
+ *                  reference "fast_float32" sampling); fixed pose.
+ *  DPT_ARITH_CELLS FP64 cell-Gauss integration: the clipped ray is split at every interpolation
+ *                  plane and each cubic segment integrated exactly with two Gauss nodes (the
+ *                  reference integration="cell_gauss", kernels/projection.py:522-746); `samples`
+ *                  is ignored. */
 enum {
     DPT_ARITH_F32 = 0,
     DPT_ARITH_F64 = 1,
-    DPT_ARITH_F32C = 2
+    DPT_ARITH_F32C = 2,
+    DPT_ARITH_MIXED = 3,
+    DPT_ARITH_FAST = 4,
+    DPT_ARITH_CELLS = 5
+};
+
+/* Field value domain (reference ProjectionSpec.field_domain). */
+enum {
+    DPT_DOMAIN_PHYSICAL = 0, /* attenuation: finite and non-negative (status bit 8 otherwise) */
+    DPT_DOMAIN_SIGNED = 1    /* signed_linear: any finite value (e.g. a linearised increment) */
 };
 
 /* How rays are described. */
@@ -87,8 +106,10 @@ enum {
 #define DPT_VIEW_MODE_WORD 18
 
 /* Field layouts read by the sampling kernels.
- *  DPT_LAYOUT_REPLICATED  corner-replicated copy written by dpt_b200_prepare_field (default):
- *                         FP32 storage 16 bytes per voxel, FP16/BF16 storage 16 bytes per voxel.
+ *  DPT_LAYOUT_REPLICATED  copy written by dpt_b200_prepare_field (default): the cell's eight
+ *                         FP32 polynomial coefficients (32 bytes per voxel) for DPT_ARITH_F32C,
+ *                         else an FP32 corner quad (16 bytes per voxel) decoded from any
+ *                         storage type.
  *  DPT_LAYOUT_DIRECT      eight gathers per sample straight from the caller's FP32 field;
  *                         `packed` then points at the field itself (no copy, FP32 only). */
 enum {
@@ -129,6 +150,8 @@ typedef struct dpt_problem {
     int32_t layout;         /* DPT_LAYOUT_*: how the sampling kernels read the field */
     int32_t block_cols;     /* panels: detector columns per 256-ray block tile: 8, 16, 32 or 64
                                (the tile is then 32, 16, 8 or 4 rows high); 0 selects 16 */
+    int32_t field_domain;   /* DPT_DOMAIN_*: which field values prepare_field accepts */
+    int32_t reserved;       /* 0 */
     double object_to_grid[9]; /* diag(1/h) G^T, row-major: grid index = M (x_object - origin) */
     double grid_origin[3];    /* object mm of sample (0,0,0) */
 } dpt_problem;

@@ -17,7 +17,7 @@ import numpy as np
 from . import build as _build
 
 F32, F64, F16, BF16 = 0, 1, 2, 3
-ARITH_F32, ARITH_F64, ARITH_F32C = 0, 1, 2
+ARITH_F32, ARITH_F64, ARITH_F32C, ARITH_MIXED, ARITH_FAST, ARITH_CELLS = 0, 1, 2, 3, 4, 5
 RAYS_PANELS, RAYS_BUNDLE = 0, 1
 VJP_VOLUME, VJP_POSE12, VJP_POSE6, VJP_PER_RAY6 = 1, 2, 4, 8
 
@@ -37,6 +37,8 @@ class _Problem(ctypes.Structure):
         ("image_dtype", ctypes.c_int32),
         ("layout", ctypes.c_int32),
         ("block_cols", ctypes.c_int32),
+        ("field_domain", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
         ("object_to_grid", ctypes.c_double * 9),
         ("grid_origin", ctypes.c_double * 3),
     ]
@@ -156,9 +158,10 @@ def vjp(plan, field, poses, cotangent, *, samples: int, flags: int, arith: int =
     return volume, pose, status
 
 
-def check_field(field: np.ndarray, field_dtype: int = F32) -> int:
+def check_field(field: np.ndarray, field_dtype: int = F32, domain: int = 0) -> int:
     p = _Problem()
     p.field_dtype = field_dtype
+    p.field_domain = domain
     data = _field_array(field, field_dtype)
     return library().oracle_check_field(ctypes.byref(p), _ptr(data), data.size)
 

@@ -343,6 +343,28 @@ static float corner_weight32(const float* fraction, int corner)
     return (f[0] * f[1]) * f[2];
 }
 
+/* MIXED / FAST sample of one FP32 point (kernels/projection.py:326-352): zero outside the
+ * support; else the FP32 clamped coordinates and corner weights, and the corner sum in FP64
+ * (MIXED, fma(w, v, value)) or FP32 (FAST, fmaf(w, v, value)) from zero. */
+static double sample_mixed32(const dpt_problem* p, const void* field, const float* q, const int* shape)
+{
+    if (!inside32(q, shape)) return 0.0;
+    int lower[3];
+    float f[3], slope[3];
+    coordinates32(q, shape, lower, f, slope);
+    if (p->arith == DPT_ARITH_FAST) {
+        float value = 0.0f;
+        for (int c = 0; c < 8; ++c)
+            value = fmaf(corner_weight32(f, c), field_value(p, field, corner_index(lower, shape, c)), value);
+        return (double)value;
+    }
+    double value = 0.0;
+    for (int c = 0; c < 8; ++c)
+        value = fma((double)corner_weight32(f, c), (double)field_value(p, field, corner_index(lower, shape, c)),
+                    value);
+    return value;
+}
+
 /* sample_pose_field, kernels/projection_fp32.py:180-209 (value and grid slope). */
 static float sample32(const dpt_problem* p, const void* field, const float* q, const int* shape,
                       float* gradient)
@@ -698,6 +720,321 @@ static void forward_action32c(void* context, const run32c_t* run)
     kahan_add32(&ctx->total, run_sum32c(run, &o));
 }
 
+/* ------------------------------------------------------ FP64 cell-Gauss integration
+ * kernels/projection.py:522-746: the clipped ray [lower, upper] is split at every
+ * interpolation plane (integer grid coordinates 0..n-1 on each axis; the half-cell margins
+ * are segments of their own) and each segment, on which the field is a cubic in t, is
+ * integrated exactly with the two-node Gauss rule. */
+
+typedef struct {
+    int plane[3], step[3];
+    double next[3], inverse[3];
+} cells_t;
+
+typedef struct {
+    double end, radius, first_position, second_position;
+    double first_point[3], second_point[3];
+    int lower[3];
+    int shared;
+} segment_t;
+
+/* kernels/projection.py:530-541: cached reciprocal with one FMA correction */
+static double crossing_quotient(double delta, double direction, double inverse)
+{
+    if (inverse == 0.0) return delta / direction;
+    const double quotient = delta * inverse;
+    if (!isfinite(quotient) || fabs(quotient) < 2.2250738585072014e-308) return delta / direction;
+    return fma(fma(-quotient, direction, delta), inverse, quotient);
+}
+
+/* :543-556 */
+static double cell_crossing(const ray64_t* r, int axis, int plane, const int* shape, double upper,
+                            double inverse)
+{
+    if (r->direction[axis] == 0.0 || plane < 0 || plane >= shape[axis]) return upper;
+    const double c = crossing_quotient((double)plane - r->origin[axis], r->direction[axis], inverse);
+    return c < upper ? c : upper;
+}
+
+/* :559-611: next strictly forward plane per axis, half-cell edge planes included */
+static void begin_cells(const ray64_t* r, const interval64_t* iv, const int* shape, cells_t* t)
+{
+    memset(t, 0, sizeof(*t));
+    for (int a = 0; a < 3; ++a) {
+        const double entry = fma(iv->lower, r->direction[a], r->origin[a]);
+        const double v = r->direction[a];
+        if (v != 0.0) {
+            const double inverse = 1.0 / v;
+            if (isfinite(inverse) && fabs(inverse) >= 2.2250738585072014e-308 &&
+                fabs(v) >= 2.2250738585072014e-308)
+                t->inverse[a] = inverse;
+        }
+        if (v > 0.0) {
+            t->step[a] = 1;
+            const int c = (int)ceil(entry);
+            t->plane[a] = c > 0 ? c : 0;
+        } else if (v < 0.0) {
+            t->step[a] = -1;
+            const int c = (int)floor(entry);
+            t->plane[a] = c < shape[a] - 1 ? c : shape[a] - 1;
+        }
+        double crossing = cell_crossing(r, a, t->plane[a], shape, iv->upper, t->inverse[a]);
+        if (crossing <= iv->lower) {
+            t->plane[a] += t->step[a];
+            crossing = cell_crossing(r, a, t->plane[a], shape, iv->upper, t->inverse[a]);
+        }
+        t->next[a] = crossing;
+    }
+}
+
+/* :199-206 */
+static void cell_lower64(const double* q, const int* shape, int* lower)
+{
+    for (int a = 0; a < 3; ++a) {
+        const double high = (double)(shape[a] - 1);
+        const double c = q[a] < 0.0 ? 0.0 : (q[a] > high ? high : q[a]);
+        lower[a] = cell_floor(c, shape[a]);
+    }
+}
+
+/* :614-646: Gauss nodes of the segment from `start` to the nearest plane */
+static void cell_segment(const ray64_t* r, const cells_t* t, double start, const int* shape, segment_t* s)
+{
+    const double n12 = t->next[1] < t->next[2] ? t->next[1] : t->next[2];
+    s->end = t->next[0] < n12 ? t->next[0] : n12;
+    s->radius = (s->end - start) * 0.5;
+    const double centre = start + s->radius;
+    const double offset = s->radius / sqrt(3.0);
+    s->first_position = centre - offset;
+    s->second_position = centre + offset;
+    double centre_point[3];
+    for (int a = 0; a < 3; ++a) {
+        s->first_point[a] = fma(s->first_position, r->direction[a], r->origin[a]);
+        s->second_point[a] = fma(s->second_position, r->direction[a], r->origin[a]);
+        centre_point[a] = fma(centre, r->direction[a], r->origin[a]);
+    }
+    cell_lower64(centre_point, shape, s->lower);
+    s->shared = 1;
+    for (int a = 0; a < 3; ++a) {
+        const double low = (double)s->lower[a], up = low + 1.0, high = (double)(shape[a] - 1);
+        const double first = s->first_point[a] < 0.0 ? 0.0 : (s->first_point[a] > high ? high : s->first_point[a]);
+        const double second = s->second_point[a] < 0.0 ? 0.0 : (s->second_point[a] > high ? high : s->second_point[a]);
+        if (first < low || second < low) s->shared = 0;
+        if (s->lower[a] < shape[a] - 2 && (first >= up || second >= up)) s->shared = 0;
+    }
+}
+
+/* :649-660: advance every axis whose plane the segment reached (ties together) */
+static void advance_cells(cells_t* t, const ray64_t* r, const int* shape, double end, double upper)
+{
+    for (int a = 0; a < 3; ++a) {
+        if (t->next[a] <= end) {
+            t->plane[a] += t->step[a];
+            t->next[a] = cell_crossing(r, a, t->plane[a], shape, upper, t->inverse[a]);
+        }
+    }
+}
+
+/* :663-674: value at a clipped endpoint, clamped into the support first */
+static double support_value(const dpt_problem* p, const void* field, const double* q, const int* shape)
+{
+    double bounded[3];
+    for (int a = 0; a < 3; ++a) {
+        const double high = (double)shape[a] - 0.5;
+        bounded[a] = q[a] < -0.5 ? -0.5 : (q[a] > high ? high : q[a]);
+    }
+    return sample64(p, field, bounded, shape, NULL);
+}
+
+/* :717-746 with the segment action :695-711: returns status bits, the integral in *out */
+static int forward_cells(const dpt_problem* p, const void* field, const ray_t* ray, double* out)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0;
+    const interval64_t* iv = &ray->iv64;
+    double integral = 0.0;
+    if (iv->upper > iv->lower) {
+        cells_t t;
+        begin_cells(&ray->r, iv, shape, &t);
+        double start = iv->lower;
+        int64_t segments = 0, limit = (int64_t)shape[0] + shape[1] + shape[2] + 1;
+        while (start < iv->upper && segments < limit) {
+            segment_t s;
+            cell_segment(&ray->r, &t, start, shape, &s);
+            if (s.end <= start) {
+                status |= 2;
+                break;
+            }
+            if (!finite3(s.first_point) || !finite3(s.second_point)) status |= 2;
+            integral = fma(s.radius, sample64(p, field, s.first_point, shape, NULL), integral);
+            integral = fma(s.radius, sample64(p, field, s.second_point, shape, NULL), integral);
+            start = s.end;
+            advance_cells(&t, &ray->r, shape, s.end, iv->upper);
+            ++segments;
+        }
+        if (start < iv->upper) status |= 2;
+        integral *= ray->r.length;
+    }
+    *out = integral;
+    if (!isfinite(p->image_dtype == DPT_F32 ? (double)(float)integral : integral)) status |= 2;
+    return status;
+}
+
+/* ((seed w0) w1) w2 with w = 1 - f for a 0 bit (scaled_corner_weight, :396-404) */
+static double scaled_corner64(const double* fraction, int corner, double seed)
+{
+    double contribution = seed;
+    for (int a = 0; a < 3; ++a) contribution *= ((corner >> a) & 1) ? fraction[a] : 1.0 - fraction[a];
+    return contribution;
+}
+
+static void fraction64(const double* q, const int* lower, const int* shape, double* fraction)
+{
+    for (int a = 0; a < 3; ++a) {
+        const double high = (double)(shape[a] - 1);
+        const double c = q[a] < 0.0 ? 0.0 : (q[a] > high ? high : q[a]);
+        fraction[a] = c - (double)lower[a];
+    }
+}
+
+/* get_scatter_field (:421-479), strict coordinates, FP32 increments */
+static int scatter_point64(const dpt_problem* p, double* gradient, const double* q, double seed)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0, lower[3];
+    if (!finite3(q)) status |= 2;
+    if (!inside64(q, shape)) return status;
+    double fraction[3];
+    cell_lower64(q, shape, lower);
+    fraction64(q, lower, shape, fraction);
+    for (int c = 0; c < 8; ++c) {
+        const float rounded = (float)scaled_corner64(fraction, c, seed);
+        if (!isfinite(rounded)) status |= 2;
+        gradient[corner_index(lower, shape, c)] += (double)rounded;
+    }
+    return status;
+}
+
+/* get_scatter_cell (:482-515): both nodes in one cell, corner terms summed in FP64 first */
+static int scatter_cell64(const dpt_problem* p, double* gradient, const segment_t* s, double seed)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0;
+    if (!finite3(s->first_point) || !finite3(s->second_point)) status |= 2;
+    double f1[3], f2[3];
+    fraction64(s->first_point, s->lower, shape, f1);
+    fraction64(s->second_point, s->lower, shape, f2);
+    const int in1 = inside64(s->first_point, shape), in2 = inside64(s->second_point, shape);
+    for (int c = 0; c < 8; ++c) {
+        const double first = scaled_corner64(f1, c, in1 ? seed : 0.0);
+        const double second = scaled_corner64(f2, c, in2 ? seed : 0.0);
+        const float rounded = (float)(first + second);
+        if (!isfinite(rounded)) status |= 2;
+        gradient[corner_index(s->lower, shape, c)] += (double)rounded;
+    }
+    return status;
+}
+
+/* Packed-12 and local-right 6 pose rows from the object-space source and direction
+ * cotangents (kernels/projection.py:1184-1210, kernels/geometry.py:39-52). */
+static void pose_rows64(const ray_t* ray, const double* sa, const double* da, double* g12, double* g6)
+{
+    if (g12) {
+        const double* wsr = ray->r.world_source_relative;
+        const double* wd = ray->r.world_direction;
+        for (int row = 0; row < 3; ++row)
+            for (int col = 0; col < 3; ++col)
+                g12[3 * row + col] = fma(wd[row], da[col], wsr[row] * sa[col]);
+        g12[12] = sa[0];
+        g12[13] = sa[1];
+        g12[14] = sa[2];
+    }
+    if (g6) {
+        const double* os = ray->r.object_source;
+        const double* od = ray->r.object_direction;
+        g6[0] = -sa[0];
+        g6[1] = -sa[1];
+        g6[2] = -sa[2];
+        g6[3] = fma(-da[2], od[1], da[1] * od[2]) + fma(-sa[2], os[1], sa[1] * os[2]);
+        g6[4] = fma(-da[0], od[2], da[2] * od[0]) + fma(-sa[0], os[2], sa[2] * os[0]);
+        g6[5] = fma(-da[1], od[0], da[0] * od[1]) + fma(-sa[1], os[0], sa[0] * os[1]);
+    }
+}
+
+/* Cell-Gauss VJP of one ray (kernels/projection.py:935-1024 and the shared tail
+ * 1152-1210): Gauss-node gradients weighted by the radius (origin) and radius x position
+ * (direction), the endpoint terms of the zero-extended support, factor = seed*length. */
+static int vjp_ray_cells(const dpt_problem* p, const void* field, const ray_t* ray, double seed,
+                         int flags, double* gradient, double* g12, double* g6)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0;
+    const int active_volume = (flags & DPT_VJP_VOLUME) != 0;
+    const int active_pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
+    const interval64_t* iv = &ray->iv64;
+    double span = iv->upper - iv->lower;
+    if (!isfinite(seed)) status |= 2;
+    if (seed == 0.0) span = 0.0;
+    if (!(span > 0.0)) return status;
+    const double factor = seed * ray->r.length;
+    double og[3] = {0.0, 0.0, 0.0}, dg[3] = {0.0, 0.0, 0.0};
+    cells_t t;
+    begin_cells(&ray->r, iv, shape, &t);
+    double start = iv->lower;
+    int64_t segments = 0, limit = (int64_t)shape[0] + shape[1] + shape[2] + 1;
+    while (start < iv->upper && segments < limit) {
+        segment_t s;
+        cell_segment(&ray->r, &t, start, shape, &s);
+        if (s.end <= start) {
+            status |= 2;
+            break;
+        }
+        if (!finite3(s.first_point) || !finite3(s.second_point)) status |= 2;
+        if (active_pose) {
+            double g1[3], g2[3];
+            sample64(p, field, s.first_point, shape, g1);
+            sample64(p, field, s.second_point, shape, g2);
+            const double r1 = s.radius * s.first_position, r2 = s.radius * s.second_position;
+            for (int a = 0; a < 3; ++a) {
+                og[a] = fma(s.radius, g1[a], og[a]);
+                og[a] = fma(s.radius, g2[a], og[a]);
+                dg[a] = fma(r1, g1[a], dg[a]);
+                dg[a] = fma(r2, g2[a], dg[a]);
+            }
+        }
+        if (active_volume) {
+            const double volume_factor = factor * s.radius;
+            if (s.shared) {
+                status |= scatter_cell64(p, gradient, &s, volume_factor);
+            } else {
+                status |= scatter_point64(p, gradient, s.first_point, volume_factor);
+                status |= scatter_point64(p, gradient, s.second_point, volume_factor);
+            }
+        }
+        start = s.end;
+        advance_cells(&t, &ray->r, shape, s.end, iv->upper);
+        ++segments;
+    }
+    if (start < iv->upper) status |= 2;
+    if (!active_pose) return status;
+    double lower_point[3], upper_point[3];
+    for (int a = 0; a < 3; ++a) {
+        lower_point[a] = fma(iv->lower, ray->r.direction[a], ray->r.origin[a]);
+        upper_point[a] = fma(iv->upper, ray->r.direction[a], ray->r.origin[a]);
+    }
+    const double lower_value = support_value(p, field, lower_point, shape);
+    const double upper_value = support_value(p, field, upper_point, shape);
+    for (int a = 0; a < 3; ++a) {
+        og[a] = og[a] + fma(-lower_value, iv->lower_origin[a], upper_value * iv->upper_origin[a]);
+        dg[a] = dg[a] + fma(-lower_value, iv->lower_direction[a], upper_value * iv->upper_direction[a]);
+    }
+    double sa[3], da[3];
+    matvec_t(p->object_to_grid, og, sa);
+    matvec_t(p->object_to_grid, dg, da);
+    for (int a = 0; a < 3; ++a) {
+        sa[a] = factor * sa[a];
+        da[a] = factor * da[a];
+    }
+    pose_rows64(ray, sa, da, g12, g6);
+    return status;
+}
+
 /* ------------------------------------------------------------------ forward */
 
 /* One ray's optical depth; returns status bits. */
@@ -734,6 +1071,29 @@ static int forward_ray(const dpt_problem* p, const void* field, const ray_t* ray
                 if (!finite3(q)) status |= 2;
                 integral += sample64(p, field, q, shape, NULL);
             }
+            integral *= ray->r.length * step;
+        }
+        *out = integral;
+        if (!isfinite(p->image_dtype == DPT_F32 ? (double)(float)integral : integral)) status |= 2;
+    } else if (p->arith == DPT_ARITH_CELLS) {
+        status |= forward_cells(p, field, ray, out);
+    } else if (p->arith == DPT_ARITH_MIXED || p->arith == DPT_ARITH_FAST) {
+        /* kernels/projection.py:296-392 (mixed_coordinates, mixed_corner_weight,
+         * sample_mixed_field / sample_float32_field, begin_midpoints, mixed_point_fma) with the
+         * midpoint integrator 770-799: FP32 points and weights; MIXED sums w*v in FP64, FAST
+         * in an FP32 fmaf cell sum promoted to the FP64 ray sum. */
+        const interval64_t* iv = &ray->iv64;
+        double integral = 0.0;
+        if (iv->upper > iv->lower) {
+            float entry[3], stepv[3];
+            march32c(ray, S, entry, stepv);
+            for (int i = 0; i < S; ++i) {
+                float q[3];
+                point32c(entry, stepv, i, q);
+                if (!finite3f(q)) status |= 2;
+                integral += sample_mixed32(p, field, q, shape);
+            }
+            double step = (iv->upper - iv->lower) / (double)S;
             integral *= ray->r.length * step;
         }
         *out = integral;
@@ -844,7 +1204,7 @@ int oracle_counts(const dpt_problem* p, const double* poses, const double* view_
                     count += inside32(q, shape);
                 }
             }
-        } else if (ray.valid && p->arith == DPT_ARITH_F64) {
+        } else if (ray.valid && (p->arith == DPT_ARITH_F64 || p->arith == DPT_ARITH_CELLS)) {
             lo = ray.iv64.lower;
             hi = ray.iv64.upper;
             if (hi > lo) {
@@ -1055,6 +1415,37 @@ static int vjp_ray_f32(const dpt_problem* p, const void* field, const ray_t* ray
 
 /* One ray of the strict FP64 joint VJP (midpoint), kernels/projection.py:922-1217, with
  * FP32-rounded volume increments (scatter_realised, kernels/projection.py:407-430). */
+/* MIXED / FAST volume VJP (fixed pose), kernels/projection.py:1026-1106 with the mixed scatter
+ * of get_scatter_field (:431-479): volume_factor = seed*length*span/S in FP64; every inside
+ * sample adds, per corner, the FP32 rounding of volume_factor * (double)w_c, w_c the FP32
+ * corner weight of the forward. */
+static int vjp_ray_mixed(const dpt_problem* p, const ray_t* ray, double seed, scatter_t* sc)
+{
+    int shape[3] = {p->nx, p->ny, p->nz}, status = 0, S = p->samples;
+    const interval64_t* iv = &ray->iv64;
+    double span = iv->upper - iv->lower;
+    if (!isfinite(seed)) status |= 2;
+    if (seed == 0.0) span = 0.0;
+    if (!(span > 0.0)) return status;
+    double volume_factor = seed * ray->r.length * span / (double)S;
+    float entry[3], stepv[3];
+    march32c(ray, S, entry, stepv);
+    for (int i = 0; i < S; ++i) {
+        float q[3], f[3], slope[3];
+        int lower[3];
+        point32c(entry, stepv, i, q);
+        if (!finite3f(q)) status |= 2;
+        if (!inside32(q, shape)) continue;
+        coordinates32(q, shape, lower, f, slope);
+        for (int c = 0; c < 8; ++c) {
+            float rounded = (float)(volume_factor * (double)corner_weight32(f, c));
+            if (!isfinite(rounded)) status |= 2;
+            sc->gradient[corner_index(lower, shape, c)] += (double)rounded;
+        }
+    }
+    return status;
+}
+
 static int vjp_ray_f64(const dpt_problem* p, const void* field, const ray_t* ray, double seed,
                        int flags, scatter_t* sc, double* g12, double* g6)
 {
@@ -1449,6 +1840,12 @@ int oracle_vjp(const dpt_problem* p, const double* poses, const double* view_tab
                 bits = vjp_ray_f64(p, field, &ray, seed, flags, &sc,
                                    (flags & DPT_VJP_POSE12) ? g12 : NULL,
                                    (flags & (DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) ? g6 : NULL);
+            } else if (p->arith == DPT_ARITH_MIXED || p->arith == DPT_ARITH_FAST) {
+                bits = (flags & DPT_VJP_VOLUME) ? vjp_ray_mixed(p, &ray, seed, &sc) : 0;
+            } else if (p->arith == DPT_ARITH_CELLS) {
+                bits = vjp_ray_cells(p, field, &ray, seed, flags, sc.gradient,
+                                     (flags & DPT_VJP_POSE12) ? g12 : NULL,
+                                     (flags & (DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) ? g6 : NULL);
             } else {
                 bits = vjp_ray_f32c(p, field, &ray, seed, flags, &sc,
                                     (flags & DPT_VJP_POSE12) ? g12 : NULL,
@@ -1514,7 +1911,7 @@ int oracle_check_field(const dpt_problem* p, const void* field, int64_t voxels)
 {
     for (int64_t v = 0; v < voxels; ++v) {
         float value = field_value(p, field, v);
-        if (!isfinite(value) || value < 0.0f) return 8;
+        if (!isfinite(value) || (p->field_domain != DPT_DOMAIN_SIGNED && value < 0.0f)) return 8;
     }
     return 0;
 }

@@ -20,7 +20,8 @@ from scenes import cone_scene, fp32_fixture, identity_poses, mixed_panels, poses
 
 pytestmark = pytest.mark.gpu
 
-ARITH = {"float32": O.ARITH_F32, "float64": O.ARITH_F64, "compensated": O.ARITH_F32C}
+ARITH = {"float32": O.ARITH_F32, "float64": O.ARITH_F64, "compensated": O.ARITH_F32C,
+         "mixed_float32": O.ARITH_MIXED, "fast_float32": O.ARITH_FAST, "cell_gauss": O.ARITH_CELLS}
 
 
 def rel_l2(a, b):
@@ -29,9 +30,13 @@ def rel_l2(a, b):
 
 
 def workspace(grid, geometry, samples, sampling="float32", precision="float32", storage="float32",
-              layout="replicated", widen=None):
+              layout="replicated", widen=None, active_pose=True, domain="physical"):
+    integration = "midpoint"
+    if sampling == "cell_gauss":
+        sampling, integration = "float64", "cell_gauss"
     spec = ProjectionSpec(samples, precision=precision, sampling_precision=sampling,
-                          storage_precision=storage, layout=layout, widen_views=widen)
+                          storage_precision=storage, layout=layout, widen_views=widen,
+                          integration=integration, active_pose=active_pose, field_domain=domain)
     return ProjectionWorkspace(plan_rays(grid, geometry), spec, "cuda:0")
 
 
@@ -178,3 +183,92 @@ def test_block_tile_shape_changes_no_result(block_cols):
     v1, p1 = tuned.vjp(field, pose, cot, volume=True, pose="matrix")
     assert rel_l2(v1.cpu().numpy(), v0.cpu().numpy()) < 1e-6
     torch.testing.assert_close(p1, p0, rtol=1e-10, atol=1e-13)
+
+
+# ---------------------------------------------------- reference sampling options
+
+@pytest.mark.parametrize("sampling", ["mixed_float32", "fast_float32", "cell_gauss"])
+@pytest.mark.parametrize("precision", ["float32", "float64"])
+def test_reference_sampling_options_forward_and_counts_bit_exact(sampling, precision):
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views), seed=5)
+    ws = workspace(grid, geometry, 61, sampling, precision, active_pose=sampling == "cell_gauss")
+    field, pose = device_inputs(values, poses)
+    image = ws.forward(field, pose).cpu().numpy().reshape(-1)
+    expected, status = O.forward(ws.plan, values, poses, samples=61, arith=ARITH[sampling],
+                                 image_dtype=O.F64 if precision == "float64" else O.F32)
+    assert not status.any()
+    np.testing.assert_array_equal(image, expected)
+    lower, upper, realised = (t.cpu().numpy() for t in ws.counts(pose))
+    e_lower, e_upper, e_realised = O.counts(ws.plan, poses, samples=61, arith=ARITH[sampling])
+    np.testing.assert_array_equal(lower, e_lower)
+    np.testing.assert_array_equal(upper, e_upper)
+    np.testing.assert_array_equal(realised, e_realised)
+
+
+@pytest.mark.parametrize("sampling", ["mixed_float32", "fast_float32"])
+def test_fixed_pose_samplings_volume_vjp_match_oracle(sampling):
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views), seed=6)
+    ws = workspace(grid, geometry, 53, sampling, "float64", active_pose=False, widen=3)
+    field, pose = device_inputs(values, poses)
+    seed = np.random.default_rng(4).uniform(-1.0, 1.0, ws.plan.rays)
+    cot = torch.tensor(seed, device="cuda:0").reshape(ws.plan.image_shape)
+    volume, _ = ws.vjp(field, pose, cot, volume=True, pose=None)
+    e_volume, _, status = O.vjp(ws.plan, values, poses, seed, samples=53, flags=O.VJP_VOLUME,
+                                arith=ARITH[sampling], image_dtype=O.F64)
+    assert not status.any()
+    assert rel_l2(volume.cpu().numpy().reshape(-1), e_volume) < 2e-6
+    with pytest.raises(Exception):
+        ws.vjp(field, pose, cot, volume=False, pose="tangent")
+
+
+@pytest.mark.parametrize("pose_form", ["matrix", "tangent"])
+def test_cell_gauss_joint_vjp_matches_oracle(pose_form):
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views), seed=7)
+    ws = workspace(grid, geometry, 1, "cell_gauss", "float64", widen=2)
+    field, pose = device_inputs(values, poses)
+    seed = np.random.default_rng(8).uniform(-1.0, 1.0, ws.plan.rays)
+    cot = torch.tensor(seed, device="cuda:0").reshape(ws.plan.image_shape)
+    volume, pose_grad = ws.vjp(field, pose, cot, volume=True, pose=pose_form)
+    flags = O.VJP_VOLUME | (O.VJP_POSE12 if pose_form == "matrix" else O.VJP_POSE6)
+    e_volume, e_pose, status = O.vjp(ws.plan, values, poses, seed, samples=1, flags=flags,
+                                     arith=O.ARITH_CELLS, image_dtype=O.F64)
+    assert not status.any()
+    assert rel_l2(volume.cpu().numpy().reshape(-1), e_volume) < 2e-6
+    np.testing.assert_allclose(pose_grad.cpu().numpy(), e_pose, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("storage", ["float16", "bfloat16"])
+@pytest.mark.parametrize("sampling", ["float64", "fast_float32", "cell_gauss"])
+def test_half_storage_under_reference_samplings_matches_oracle(storage, sampling):
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views), seed=9)
+    ws = workspace(grid, geometry, 47, sampling, "float64", storage=storage,
+                   active_pose=sampling != "fast_float32")
+    dtype = torch.float16 if storage == "float16" else torch.bfloat16
+    field, pose = device_inputs(values, poses, dtype)
+    raw = field.cpu().view(torch.int16).numpy().view(np.uint16)
+    code = O.F16 if storage == "float16" else O.BF16
+    image = ws.forward(field, pose).cpu().numpy().reshape(-1)
+    expected, _ = O.forward(ws.plan, raw, poses, samples=47, arith=ARITH[sampling], field_dtype=code,
+                            image_dtype=O.F64)
+    np.testing.assert_array_equal(image, expected)
+
+
+def test_signed_linear_domain_accepts_negative_fields():
+    from dpt_b200.contracts import TrialDomainError
+
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views), seed=10)
+    signed = values - 0.5 * values.max()
+    field, pose = device_inputs(signed, poses)
+    ws = workspace(grid, geometry, 33, "float64", "float64", domain="signed_linear")
+    image = ws.forward(field, pose).cpu().numpy().reshape(-1)
+    expected, _ = O.forward(ws.plan, signed, poses, samples=33, arith=O.ARITH_F64, image_dtype=O.F64)
+    np.testing.assert_array_equal(image, expected)
+    assert (image < 0).any()
+    physical = workspace(grid, geometry, 33, "float64", "float64")
+    with pytest.raises(TrialDomainError):
+        physical.forward(field, pose)

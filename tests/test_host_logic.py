@@ -37,8 +37,23 @@ def test_spec_contracts():
     ProjectionSpec(8, sampling_precision="compensated", storage_precision="bfloat16")
     with pytest.raises(ContractError):
         ProjectionSpec(0)
-    with pytest.raises(ContractError, match="compensated"):
+    # reference ProjectionSpec rules (python/dpt/projection.py:113-140)
+    with pytest.raises(ContractError, match="FP32 field storage"):
         ProjectionSpec(8, sampling_precision="float32", storage_precision="float16")
+    with pytest.raises(ContractError, match="fixed pose"):
+        ProjectionSpec(8, sampling_precision="mixed_float32")
+    with pytest.raises(ContractError, match="fixed pose"):
+        ProjectionSpec(8, sampling_precision="fast_float32", active_pose=False, integration="cell_gauss")
+    with pytest.raises(ContractError):
+        ProjectionSpec(8, integration="gauss")
+    with pytest.raises(ContractError):
+        ProjectionSpec(8, field_domain="negative")
+    with pytest.raises(ContractError):
+        ProjectionSpec(8, validate="sometimes")
+    assert ProjectionSpec(8, integration="cell_gauss").arith == N.ARITH_CELLS
+    assert ProjectionSpec(8, sampling_precision="fast_float32", active_pose=False).arith == N.ARITH_FAST
+    assert ProjectionSpec(8, sampling_precision="float64", storage_precision="bfloat16").field_code == N.BF16
+    assert ProjectionSpec(8, field_domain="signed_linear").domain_code == N.DOMAIN_SIGNED
     with pytest.raises(ContractError):
         ProjectionSpec(8, layout="direct", sampling_precision="compensated", storage_precision="float16")
     assert ProjectionSpec(8, sampling_precision="float64").batch_views == 2

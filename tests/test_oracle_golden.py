@@ -106,6 +106,10 @@ def test_closed_form_integrals(index):
     # fine midpoint rules converge to the exact piecewise-Gauss integral
     image, _ = O.forward(plan, values, IDENTITY, samples=4096, arith=O.ARITH_F64, image_dtype=O.F64)
     assert image[0] == pytest.approx(case["gauss"], rel=1e-5, abs=1e-9)
+    # and cell-Gauss integration is that integral (reference validation/projection.py)
+    cells, status = O.forward(plan, values, IDENTITY, samples=1, arith=O.ARITH_CELLS, image_dtype=O.F64)
+    assert not status.any()
+    assert cells[0] == pytest.approx(case["gauss"], rel=1e-12, abs=1e-14)
 
 
 def test_projector_scene_matches_reference_fp64_matrix():
@@ -141,6 +145,28 @@ def test_compensated_half_storage_matches_reference_fp32_marching_oracle(storage
     np.testing.assert_allclose(image, data[f"{storage}_image"], rtol=1e-6, atol=1e-9)
     seed = np.asarray([1.5, -0.25, 3.0])
     volume, _, _ = O.vjp(plan, bits, IDENTITY, seed, samples=samples, flags=O.VJP_VOLUME, arith=O.ARITH_F32C,
+                         field_dtype=code, image_dtype=O.F64)
+    np.testing.assert_allclose(volume, data[f"{storage}_matrix"].T @ seed, rtol=2e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("storage", ["float16", "bfloat16"])
+def test_fast_float32_half_storage_is_the_reference_fp32_marching_oracle(storage):
+    """Reference test_projection_native_storage.py:41-84 is the fast_float32 arithmetic itself
+    (FP32 marching, clamped FP32 weights, fused FP32 cell sum, FP64 ray sum): the FAST form
+    reproduces its image to FP64 rounding and its weight matrix in the volume VJP."""
+    grid, rays, data, samples = native_fixture()
+    plan = plan_rays(grid, rays)
+    bits = data[f"{storage}_bits"]
+    code = O.F16 if storage == "float16" else O.BF16
+    image, status = O.forward(plan, bits, IDENTITY, samples=samples, arith=O.ARITH_FAST, field_dtype=code,
+                              image_dtype=O.F64)
+    assert not status.any()
+    np.testing.assert_allclose(image, data[f"{storage}_image"], rtol=1e-12, atol=1e-15)
+    mixed, _ = O.forward(plan, bits, IDENTITY, samples=samples, arith=O.ARITH_MIXED, field_dtype=code,
+                         image_dtype=O.F64)
+    np.testing.assert_allclose(mixed, data[f"{storage}_image"], rtol=1e-6, atol=1e-9)
+    seed = np.asarray([1.5, -0.25, 3.0])
+    volume, _, _ = O.vjp(plan, bits, IDENTITY, seed, samples=samples, flags=O.VJP_VOLUME, arith=O.ARITH_FAST,
                          field_dtype=code, image_dtype=O.F64)
     np.testing.assert_allclose(volume, data[f"{storage}_matrix"].T @ seed, rtol=2e-6, atol=1e-7)
 
