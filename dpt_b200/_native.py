@@ -40,6 +40,9 @@ EXPORTS = (
     "dpt_b200_fold_volume",
     "dpt_b200_counts",
     "dpt_b200_pose_vjp_fixed",
+    "dpt_b200_moments_bytes",
+    "dpt_b200_forward_moments",
+    "dpt_b200_pose_from_moments",
 )
 
 
@@ -98,6 +101,9 @@ _SIGNATURES = {
     "dpt_b200_fold_volume": ([_P, _V, _V, _I, _V, _I, _I, _V, _V], ctypes.c_int),
     "dpt_b200_counts": ([_P, _R, _V, _V, _V, _V, _V], ctypes.c_int),
     "dpt_b200_pose_vjp_fixed": ([_P, _R, _V, _V, _I, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_moments_bytes": ([_P, _I], ctypes.c_size_t),
+    "dpt_b200_forward_moments": ([_P, _R, _V, _V, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_pose_from_moments": ([_P, _R, _V, _V, _I, _V, _V, _V], ctypes.c_int),
 }
 
 _lock = threading.Lock()

@@ -194,6 +194,56 @@ int dpt_b200_forward(const dpt_problem* p, const dpt_rays* r, const void* packed
     });
 }
 
+size_t dpt_b200_moments_bytes(const dpt_problem* p, int32_t view_count)
+{
+    if (check_problem(p) != DPT_OK || view_count < 1) return 0;
+    return (size_t)9 * sizeof(float) * (size_t)view_count * (size_t)p->rows * (size_t)p->cols;
+}
+
+int dpt_b200_forward_moments(const dpt_problem* p, const dpt_rays* r, const void* packed, float* image,
+                             float* moments, int32_t* status, void* stream)
+{
+    int code = check_problem(p);
+    if (code != DPT_OK) return code;
+    if ((code = check_rays(p, r)) != DPT_OK) return code;
+    if (p->arith != DPT_ARITH_F32 || p->image_dtype != DPT_F32) return DPT_E_DTYPE;
+    if (!packed || !image || !moments || !status) return DPT_E_NULL;
+    if (!aligned(packed, 16)) return DPT_E_ALIGN;
+    const int64_t rays_per_view = (int64_t)p->rows * p->cols;
+    const int64_t stride = rays_per_view * r->view_count;
+    return chunked(p, r, status, dpt::kVjpBlock, [&](const dpt::RayArgs& a, int32_t first) {
+        const int64_t offset = (int64_t)first * rays_per_view;
+        return to_code(dpt::launch_forward_moments(*p, a, packed, image + offset, moments + offset, stride,
+                                                   static_cast<cudaStream_t>(stream)));
+    });
+}
+
+int dpt_b200_pose_from_moments(const dpt_problem* p, const dpt_rays* r, const float* moments,
+                               const void* cotangent, int32_t flags, double* pose_partials,
+                               int32_t* status, void* stream)
+{
+    int code = check_problem(p);
+    if (code != DPT_OK) return code;
+    if ((code = check_rays(p, r)) != DPT_OK) return code;
+    if (p->arith != DPT_ARITH_F32) return DPT_E_DTYPE;
+    if (!moments || !cotangent || !pose_partials || !status) return DPT_E_NULL;
+    if (flags != DPT_VJP_POSE12 && flags != DPT_VJP_POSE6 && flags != DPT_VJP_PER_RAY6) return DPT_E_FLAGS;
+    const int64_t rays_per_view = (int64_t)p->rows * p->cols;
+    const int64_t stride = rays_per_view * r->view_count;
+    const size_t element = p->image_dtype == DPT_F64 ? 8 : 4;
+    int tiles_x;
+    const int tiles = dpt::tiles_per_view(*p, &tiles_x, dpt::kVjpBlock);
+    return chunked(p, r, status, dpt::kVjpBlock, [&](const dpt::RayArgs& a, int32_t first) {
+        const int64_t offset = (int64_t)first * rays_per_view;
+        const char* seed = static_cast<const char*>(cotangent) + (size_t)offset * element;
+        const int64_t per_view = (flags & DPT_VJP_PER_RAY6) ? rays_per_view * 6
+                                 : (int64_t)tiles * ((flags & DPT_VJP_POSE12) ? 12 : 6);
+        return to_code(dpt::launch_pose_from_moments(*p, a, moments + offset, stride, seed, flags,
+                                                     pose_partials + (int64_t)first * per_view,
+                                                     static_cast<cudaStream_t>(stream)));
+    });
+}
+
 int dpt_b200_vjp(const dpt_problem* p, const dpt_rays* r, const void* packed,
                  const void* cotangent, int32_t flags, float* accumulator, double* pose_partials,
                  int32_t* status, void* stream)

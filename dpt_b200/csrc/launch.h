@@ -28,6 +28,11 @@ cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower,
 cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packed,
                        const void* cotangent, int flags, float* accumulator, double* partials,
                        cudaStream_t stream);
+cudaError_t launch_forward_moments(const dpt_problem& p, const RayArgs& a, const void* packed,
+                                   float* image, float* moments, int64_t stride, cudaStream_t stream);
+cudaError_t launch_pose_from_moments(const dpt_problem& p, const RayArgs& a, const float* moments,
+                                     int64_t stride, const void* cotangent, int flags,
+                                     double* partials, cudaStream_t stream);
 cudaError_t launch_finish_pose(int view_begin, int view_count, int tiles, int components,
                                const double* partials, double* gradient, int accumulate,
                                int32_t* status, cudaStream_t stream);

@@ -98,19 +98,37 @@ __device__ __forceinline__ void pose_epilogue(const RayArgs& a, const ViewShared
     pose_rows(mode, r, vs.pose, sa, da, g);
 }
 
-template <int kArith, class Field, bool kVol, bool kPose, typename Seed>
+// Split pose VJP (FP32 arithmetic).  The pose moments of a ray (mean, sum of slopes, sum of
+// position-weighted slopes and the two clip shifts) do not depend on its cotangent, so a
+// training step can gather them during its forward pass (kStoreMoments: the kernel samples
+// once, writes the image and the nine moments and no gradient) and finish the pose VJP
+// without sampling (kLoadMoments: read the moments, apply the cotangent and the clip-face
+// chain); the volume VJP then runs alone.  The moments are the same FP32 values the joint
+// kernel forms, so every result is unchanged.
+constexpr int kJointMoments = 0, kStoreMoments = 1, kLoadMoments = 2;
+constexpr int kMomentWords = 9;  // mean, dO[3], dD[3], shift_lower, shift_upper
+
+struct MomentArgs {
+    float* moments;  // kMomentWords x stride FP32, word k of ray r at k * stride + r
+    int64_t stride;  // rays of the call
+    float* image;    // kStoreMoments: the forward image (FP32)
+};
+
+template <int kArith, class Field, bool kVol, bool kPose, typename Seed, int kMoments = kJointMoments>
 __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_MIN_BLOCKS_F32C : kArith == DPT_ARITH_F32 ? DPT_VJP_MIN_BLOCKS_F32 : DPT_VJP_MIN_BLOCKS_F64) k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
                                                 int mode, float* __restrict__ acc,
-                                                double* __restrict__ partials)
+                                                double* __restrict__ partials, MomentArgs ma)
 {
+    static_assert(kMoments == kJointMoments || (kArith == DPT_ARITH_F32 && !kVol && kPose),
+                  "split pose moments: FP32 arithmetic, pose only");
     __shared__ ViewShared vs;
     __shared__ double warp_sums[kVjpBlock / 32][12];
     // alpha_i = (i + 0.5) / S of the FP32 pose moments, each one IEEE division, tabulated
     // once per block for the first kAlphaTable samples (later samples divide directly)
-    __shared__ float alpha_table[kArith == DPT_ARITH_F32 && kPose ? kAlphaTable : 1];
+    __shared__ float alpha_table[kArith == DPT_ARITH_F32 && kPose && kMoments != kLoadMoments ? kAlphaTable : 1];
     const int view_local = blockIdx.y;
     const int view = a.view_begin + view_local;
-    if (kArith == DPT_ARITH_F32 && kPose) {
+    if (kArith == DPT_ARITH_F32 && kPose && kMoments != kLoadMoments) {
         const int n = min(a.samples, kAlphaTable);
         for (int k = threadIdx.x; k < n; k += kVjpBlock) alpha_table[k] = ((float)k + 0.5f) / (float)a.samples;
     }
@@ -123,13 +141,17 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
 #pragma unroll
     for (int k = 0; k < 12; ++k) g[k] = 0.0;
     int bits = 0;
+    float stored[kMoments == kStoreMoments ? kMomentWords : 1] = {};
+    float stored_image = 0.0f;
 
     if (active) {
         double source[3], end[3];
         ray_endpoints(a, vs.table, view, pixel, source, end);
         Ray64 r;
         ray_setup(a.grid, vs.pose, source, end, r);
-        const double seed_in = (double)cot[view_local * rays_per_view + pixel];
+        const int64_t ray_index = view_local * rays_per_view + pixel;
+        // a forward pass that stores moments has no cotangent yet: sample as for a unit seed
+        const double seed_in = kMoments == kStoreMoments ? 1.0 : (double)cot[ray_index];
         FieldDims dims;
         dims.init(a.grid);
 
@@ -153,6 +175,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
                     const bool bounded = isfinite(vf) && fabsf(vf) <= 1.0f;
                     float mean = 0.0f, dO[3] = {0.0f, 0.0f, 0.0f}, dD[3] = {0.0f, 0.0f, 0.0f};
                     float sl = 0.0f, su = 0.0f;
+                    bool trailing_zero = false;
                     float cs[8];
 #pragma unroll
                     for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
@@ -276,14 +299,41 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
 #pragma unroll 2
                         for (int i = ifirst; i <= ilast; ++i) visit(i, 2, bounded_tag);
                         for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1, bounded_tag);
+                        trailing_zero = last < S - 1;
                     }
                     };
-                    if (bounded)
+                    if constexpr (kMoments == kLoadMoments) {
+                        const float* m = ma.moments + ray_index;
+                        mean = m[0];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            dO[k] = m[(1 + k) * ma.stride];
+                            dD[k] = m[(4 + k) * ma.stride];
+                        }
+                        sl = m[7 * ma.stride];
+                        su = m[8 * ma.stride];
+                    } else if (bounded) {
                         march(std::true_type{});
-                    else
+                    } else {
                         march(std::false_type{});
+                    }
                     if (kVol && pending >= 0) flush_cell(acc, pending, cs);
-                    if (kPose) {
+                    if constexpr (kMoments == kStoreMoments) {
+                        // the forward image: the same serial sum the forward kernel forms (a
+                        // trailing zero sample only turns -0 into +0), scaled by length*step
+                        float total = trailing_zero ? mean + 0.0f : mean;
+                        total = total * physical_step;
+                        if (!isfinite(total)) bits |= 2;
+                        stored_image = total;
+                        stored[0] = mean;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            stored[1 + k] = dO[k];
+                            stored[4 + k] = dD[k];
+                        }
+                        stored[7] = sl;
+                        stored[8] = su;
+                    } else if (kPose) {
                         float lo_o[3], lo_d[3], up_o[3], up_d[3];
                         iv.lower_gradients(lo_o, lo_d);
                         iv.upper_gradients(up_o, up_d);
@@ -866,6 +916,16 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
         }
     }
 
+    if constexpr (kMoments == kStoreMoments) {
+        if (active) {
+            const int64_t ray_index = view_local * rays_per_view + pixel;
+            ma.image[ray_index] = stored_image;
+#pragma unroll
+            for (int k = 0; k < kMomentWords; ++k) ma.moments[k * ma.stride + ray_index] = stored[k];
+        }
+        if (bits) atomicOr(a.status + view, bits);
+        return;
+    }
     if (kPose) {
         if (mode < 0) {
             if (active) {
@@ -913,14 +973,14 @@ cudaError_t vjp_with(const RayArgs& a, const Field& f, const Seed* cot, int flag
     if constexpr (kArith == DPT_ARITH_MIXED || kArith == DPT_ARITH_FAST) {
         // fixed-pose forms: the C ABI admits the volume cotangent only
         if (pose || !volume) return cudaErrorInvalidValue;
-        k_vjp<kArith, Field, true, false, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+        k_vjp<kArith, Field, true, false, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials, MomentArgs{});
     } else {
         if (volume && pose)
-            k_vjp<kArith, Field, true, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+            k_vjp<kArith, Field, true, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials, MomentArgs{});
         else if (volume)
-            k_vjp<kArith, Field, true, false, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+            k_vjp<kArith, Field, true, false, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials, MomentArgs{});
         else
-            k_vjp<kArith, Field, false, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials);
+            k_vjp<kArith, Field, false, true, Seed><<<grid, kVjpBlock, 0, stream>>>(a, f, cot, mode, acc, partials, MomentArgs{});
     }
     return cudaGetLastError();
 }
@@ -964,6 +1024,42 @@ cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packe
     };
     if (p.layout == DPT_LAYOUT_DIRECT) return run(PlainF32{static_cast<const float*>(packed), p.nx, p.ny, p.nz});
     return run(QuadF32{static_cast<const float4*>(packed), p.nx, p.ny, p.nz});
+}
+
+// Forward image plus the pose moments of every ray (FP32 arithmetic; see kStoreMoments).
+cudaError_t launch_forward_moments(const dpt_problem& p, const RayArgs& a, const void* packed,
+                                   float* image, float* moments, int64_t stride, cudaStream_t stream)
+{
+    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const MomentArgs ma{moments, stride, image};
+    if (p.layout == DPT_LAYOUT_DIRECT) {
+        PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
+        k_vjp<DPT_ARITH_F32, PlainF32, false, true, float, kStoreMoments>
+            <<<grid, kVjpBlock, 0, stream>>>(a, f, nullptr, 6, nullptr, nullptr, ma);
+    } else {
+        QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
+        k_vjp<DPT_ARITH_F32, QuadF32, false, true, float, kStoreMoments>
+            <<<grid, kVjpBlock, 0, stream>>>(a, f, nullptr, 6, nullptr, nullptr, ma);
+    }
+    return cudaGetLastError();
+}
+
+// Pose VJP from stored moments: no sampling, the field is not read.
+cudaError_t launch_pose_from_moments(const dpt_problem& p, const RayArgs& a, const float* moments,
+                                     int64_t stride, const void* cotangent, int flags,
+                                     double* partials, cudaStream_t stream)
+{
+    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const int mode = (flags & DPT_VJP_POSE12) ? 12 : ((flags & DPT_VJP_PER_RAY6) ? -6 : 6);
+    const MomentArgs ma{const_cast<float*>(moments), stride, nullptr};
+    const PlainF32 none{nullptr, p.nx, p.ny, p.nz};
+    if (p.image_dtype == DPT_F64)
+        k_vjp<DPT_ARITH_F32, PlainF32, false, true, double, kLoadMoments><<<grid, kVjpBlock, 0, stream>>>(
+            a, none, static_cast<const double*>(cotangent), mode, nullptr, partials, ma);
+    else
+        k_vjp<DPT_ARITH_F32, PlainF32, false, true, float, kLoadMoments><<<grid, kVjpBlock, 0, stream>>>(
+            a, none, static_cast<const float*>(cotangent), mode, nullptr, partials, ma);
+    return cudaGetLastError();
 }
 
 }  // namespace dpt

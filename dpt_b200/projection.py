@@ -271,6 +271,8 @@ class ProjectionWorkspace:
         self._accumulator: torch.Tensor | None = None
         self._total: torch.Tensor | None = None
         self._partials: torch.Tensor | None = None
+        self._moments: torch.Tensor | None = None
+        self._moments_for: tuple | None = None
         # Optional instrumentation: a list receiving (name, view_begin, view_count,
         # start_event, end_event) per C-ABI call, and a count of C-ABI calls.
         self.launch_log: list | None = None
@@ -283,7 +285,7 @@ class ProjectionWorkspace:
 
     def scratch_bytes(self) -> int:
         total = 0
-        for tensor in (self._packed, self._accumulator, self._total, self._partials):
+        for tensor in (self._packed, self._accumulator, self._total, self._partials, self._moments):
             if tensor is not None:
                 total += tensor.numel() * tensor.element_size()
         return total
@@ -292,6 +294,7 @@ class ProjectionWorkspace:
         """Drop the cached field copy and gradient scratch (allocated again on demand)."""
         self._packed = self._packed_for = None
         self._accumulator = self._total = self._partials = None
+        self._moments = self._moments_for = None
 
     def _bytes(self, size: int) -> torch.Tensor:
         # 256-byte aligned storage from the caching allocator
@@ -434,9 +437,33 @@ class ProjectionWorkspace:
             raise first
 
     # ------------------------------------------------------------ compute
+    # Largest stored pose moments (FP32 words) a workspace keeps between a forward and its VJP.
+    MOMENT_BYTES_LIMIT = 16 << 30
+
+    def moments_supported(self) -> bool:
+        """Whether a forward can store the pose moments for a later pose VJP (FP32 arithmetic
+        and images, within MOMENT_BYTES_LIMIT)."""
+        return (self.spec.arith == N.ARITH_F32 and self.spec.image_code == N.F32 and
+                N.library().dpt_b200_moments_bytes(self.problem, self.views) <= self.MOMENT_BYTES_LIMIT)
+
+    def _moments_match(self, field: torch.Tensor, poses: torch.Tensor) -> bool:
+        """Whether the stored moments belong to these inputs.  The workspace holds the
+        inputs of the forward that stored them, so equal storage pointers cannot come from
+        another tensor reusing the memory; equal version counters mean unchanged contents."""
+        kept = self._moments_for
+        if kept is None:
+            return False
+        f0, p0, fv, pv = kept
+        return (field.data_ptr() == f0.data_ptr() and poses.data_ptr() == p0.data_ptr()
+                and field._version == fv and poses._version == pv)
+
     def forward(self, field: torch.Tensor, poses: torch.Tensor, out: torch.Tensor | None = None,
-                *, checked: bool = True) -> torch.Tensor:
-        """Optical depth ``(views, rows, cols)`` (bundles: ``(rays,)``)."""
+                *, checked: bool = True, moments: bool = False) -> torch.Tensor:
+        """Optical depth ``(views, rows, cols)`` (bundles: ``(rays,)``).
+
+        ``moments=True`` (FP32 arithmetic) also stores each ray's pose moments, so that a
+        following ``vjp`` with the same field and poses forms the pose gradient without
+        sampling again; the image is identical either way."""
         with self.lock, torch.cuda.device(self.device):
             field = self.check_field(field)
             poses = self.check_poses(poses)
@@ -446,9 +473,20 @@ class ProjectionWorkspace:
                   or out.device != self.device or not out.is_contiguous()):
                 raise ContractError("out must match the projector's shape, dtype and input device")
             packed = self.prepare_field(field, poses)
-            self._run("forward", lambda: N.library().dpt_b200_forward(self.problem, self.rays(poses), packed.data_ptr(),
-                                             out.data_ptr(), self.status.data_ptr(),
-                                             _stream(self.device)))
+            self._moments_for = None
+            if moments and self.moments_supported():
+                lib = N.library()
+                size = lib.dpt_b200_moments_bytes(self.problem, self.views)
+                if self._moments is None or self._moments.numel() * 4 < size:
+                    self._moments = torch.empty(size // 4, dtype=torch.float32, device=self.device)
+                self._run("forward", lambda: lib.dpt_b200_forward_moments(
+                    self.problem, self.rays(poses), packed.data_ptr(), out.data_ptr(),
+                    self._moments.data_ptr(), self.status.data_ptr(), _stream(self.device)))
+                self._moments_for = (field, poses, field._version, poses._version)
+            else:
+                self._run("forward", lambda: N.library().dpt_b200_forward(self.problem, self.rays(poses), packed.data_ptr(),
+                                                 out.data_ptr(), self.status.data_ptr(),
+                                                 _stream(self.device)))
             if checked and self.spec.validate != "never":
                 self.consume_status()
             return out
@@ -475,6 +513,12 @@ class ProjectionWorkspace:
             elif pose == "tangent":
                 flags |= N.VJP_POSE6
                 components = 6
+            # pose moments stored by the forward of these same inputs: the pose VJP needs no
+            # sampling and the sampling pass scatters the volume cotangent alone
+            split = bool(components) and self._moments_match(field, poses)
+            if split:
+                flags &= N.VJP_VOLUME
+                self._moments_for = None  # consumed: release the forward's inputs
             accumulator = self.accumulator().data_ptr() if volume else None
             partials = self.partials() if components else None
             gradient = (torch.empty(self.plan.grid.shape, dtype=volume_dtype, device=self.device)
@@ -484,11 +528,16 @@ class ProjectionWorkspace:
             batch = self.spec.batch_views if volume else self.views
             rays_per_view = self.plan.rays_per_view
             element = cot.element_size()
-            for first in range(0, self.views, batch):
+            if split:
+                self._run("pose_from_moments", lambda: lib.dpt_b200_pose_from_moments(
+                    self.problem, self.rays(poses), self._moments.data_ptr(), cot.data_ptr(),
+                    N.VJP_POSE12 if components == 12 else N.VJP_POSE6, partials.data_ptr(),
+                    self.status.data_ptr(), stream))
+            for first in range(0, self.views if volume else 0 if split else self.views, batch):
                 count = min(batch, self.views - first)
                 seed_ptr = cot.data_ptr() + first * rays_per_view * element
                 part_ptr = None
-                if partials is not None:
+                if partials is not None and not split:
                     tiles = lib.dpt_b200_pose_partials_bytes(self.problem, 1) // (12 * 8)
                     part_ptr = partials.data_ptr() + first * tiles * components * 8
                 self._run("vjp", lambda: lib.dpt_b200_vjp(self.problem, self.rays(poses, first, count), packed.data_ptr(),

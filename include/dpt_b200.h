@@ -196,6 +196,24 @@ int dpt_b200_vjp(const dpt_problem* problem, const dpt_rays* rays, const void* p
                  const void* cotangent, int32_t flags, float* accumulator,
                  double* pose_partials, int32_t* status, void* stream);
 
+/* Split pose VJP (DPT_ARITH_F32, FP32 images).  A ray's pose moments (its sample sum, sums of
+ * the grid slopes and of the position-weighted slopes, and the two clip shifts: 9 FP32
+ * words) do not depend on its cotangent.  dpt_b200_forward_moments writes the forward image
+ * (identical to dpt_b200_forward) and stores the moments, word k of ray i of the call at
+ * moments[k * view_count*rows*cols + i] (dpt_b200_moments_bytes);
+ * dpt_b200_pose_from_moments then forms the pose partials of dpt_b200_vjp for one pose
+ * form (DPT_VJP_POSE12, POSE6 or PER_RAY6) from the moments and the cotangent without
+ * sampling the field, so a training step samples twice (forward with moments, volume VJP)
+ * instead of three times.  Results equal those of dpt_b200_vjp with the same flags.
+ * Replaces the pose part of python/dpt/projection.py:871-1018 (projection_vjp), kernels
+ * python/dpt/kernels/projection_fp32.py:443-458 and 549-615. */
+size_t dpt_b200_moments_bytes(const dpt_problem* problem, int32_t view_count);
+int dpt_b200_forward_moments(const dpt_problem* problem, const dpt_rays* rays, const void* packed,
+                             float* image, float* moments, int32_t* status, void* stream);
+int dpt_b200_pose_from_moments(const dpt_problem* problem, const dpt_rays* rays, const float* moments,
+                               const void* cotangent, int32_t flags, double* pose_partials,
+                               int32_t* status, void* stream);
+
 /* Reduce the pose partials of a dpt_b200_vjp call over views [view_begin, view_begin +
  * view_count) in a fixed FP64 order into `pose_gradient` (view_count x components,
  * components 12 or 6); accumulate != 0 adds.  Non-finite results set bit 2 of

@@ -272,3 +272,33 @@ def test_signed_linear_domain_accepts_negative_fields():
     physical = workspace(grid, geometry, 33, "float64", "float64")
     with pytest.raises(TrialDomainError):
         physical.forward(field, pose)
+
+
+@pytest.mark.parametrize("pose_form", ["matrix", "tangent"])
+@pytest.mark.parametrize("volume", [True, False])
+def test_split_pose_vjp_from_forward_moments_equals_joint_vjp(pose_form, volume):
+    """A forward that stores the pose moments writes the same image, and the VJP that then
+    forms the pose gradient from them (no second sampling pass) equals the joint VJP."""
+    grid, geometry, values = cone_scene()
+    poses = poses_for(len(geometry.views), seed=12)
+    field, pose = device_inputs(values, poses)
+    joint = workspace(grid, geometry, 53, widen=3)
+    split = workspace(grid, geometry, 53, widen=3)
+    image = joint.forward(field, pose)
+    image_m = split.forward(field, pose, moments=True)
+    torch.testing.assert_close(image_m, image, rtol=0, atol=0)
+    cot = torch.rand(image.shape, device="cuda:0") - 0.5
+    v0, p0 = joint.vjp(field, pose, cot, volume=volume, pose=pose_form)
+    v1, p1 = split.vjp(field, pose, cot, volume=volume, pose=pose_form)
+    torch.testing.assert_close(p1, p0, rtol=0, atol=0)
+    if volume:
+        assert rel_l2(v1.cpu().numpy(), v0.cpu().numpy()) < 1e-6
+    # the moments are consumed: a second VJP samples again and still agrees
+    _, p2 = split.vjp(field, pose, cot, volume=False, pose=pose_form)
+    torch.testing.assert_close(p2, p0, rtol=0, atol=0)
+    # changed poses after the forward: the stored moments are not used
+    pose.add_(0.0)
+    split.forward(field, pose, moments=True)
+    pose.mul_(1.0)  # bumps the version counter
+    _, p3 = split.vjp(field, pose, cot, volume=False, pose=pose_form)
+    torch.testing.assert_close(p3, p0, rtol=0, atol=0)
