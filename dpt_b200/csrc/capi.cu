@@ -206,7 +206,8 @@ int dpt_b200_forward_moments(const dpt_problem* p, const dpt_rays* r, const void
     int code = check_problem(p);
     if (code != DPT_OK) return code;
     if ((code = check_rays(p, r)) != DPT_OK) return code;
-    if (p->arith != DPT_ARITH_F32 || p->image_dtype != DPT_F32) return DPT_E_DTYPE;
+    if ((p->arith != DPT_ARITH_F32 && p->arith != DPT_ARITH_F32C) || p->image_dtype != DPT_F32)
+        return DPT_E_DTYPE;
     if (!packed || !image || !moments || !status) return DPT_E_NULL;
     if (!aligned(packed, 16)) return DPT_E_ALIGN;
     const int64_t rays_per_view = (int64_t)p->rows * p->cols;
@@ -225,7 +226,7 @@ int dpt_b200_pose_from_moments(const dpt_problem* p, const dpt_rays* r, const fl
     int code = check_problem(p);
     if (code != DPT_OK) return code;
     if ((code = check_rays(p, r)) != DPT_OK) return code;
-    if (p->arith != DPT_ARITH_F32) return DPT_E_DTYPE;
+    if (p->arith != DPT_ARITH_F32 && p->arith != DPT_ARITH_F32C) return DPT_E_DTYPE;
     if (!moments || !cotangent || !pose_partials || !status) return DPT_E_NULL;
     if (flags != DPT_VJP_POSE12 && flags != DPT_VJP_POSE6 && flags != DPT_VJP_PER_RAY6) return DPT_E_FLAGS;
     const int64_t rays_per_view = (int64_t)p->rows * p->cols;

@@ -106,7 +106,10 @@ __device__ __forceinline__ void pose_epilogue(const RayArgs& a, const ViewShared
 // chain); the volume VJP then runs alone.  The moments are the same FP32 values the joint
 // kernel forms, so every result is unchanged.
 constexpr int kJointMoments = 0, kStoreMoments = 1, kLoadMoments = 2;
-constexpr int kMomentWords = 9;  // mean, dO[3], dD[3], shift_lower, shift_upper
+// FP32: mean, dO[3], dD[3], shift_lower, shift_upper; compensated: the mean's sum and
+// compensation, G[3], H[3] and whether H is the cell-run sum (to divide by S) or already
+// alpha-weighted (per-sample form)
+constexpr int kMomentWords = 9;
 
 struct MomentArgs {
     float* moments;  // kMomentWords x stride FP32, word k of ray r at k * stride + r
@@ -119,8 +122,9 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
                                                 int mode, float* __restrict__ acc,
                                                 double* __restrict__ partials, MomentArgs ma)
 {
-    static_assert(kMoments == kJointMoments || (kArith == DPT_ARITH_F32 && !kVol && kPose),
-                  "split pose moments: FP32 arithmetic, pose only");
+    static_assert(kMoments == kJointMoments ||
+                      ((kArith == DPT_ARITH_F32 || kArith == DPT_ARITH_F32C) && !kVol && kPose),
+                  "split pose moments: FP32 or compensated arithmetic, pose only");
     __shared__ ViewShared vs;
     __shared__ double warp_sums[kVjpBlock / 32][12];
     // alpha_i = (i + 0.5) / S of the FP32 pose moments, each one IEEE division, tabulated
@@ -742,7 +746,11 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
                         if (!finite) bits |= 2;
                         flush_cell(acc, cell, corner);
                     };
-                    if (moderate(entry, sv)) {
+                    float words[kMomentWords] = {};
+                    if constexpr (kMoments == kLoadMoments) {
+#pragma unroll
+                        for (int k = 0; k < kMomentWords; ++k) words[k] = ma.moments[k * ma.stride + ray_index];
+                    } else if (moderate(entry, sv)) {
                         // segment form: every cell run in closed form
                         int first, last;
                         inside_run(S, [&](int i) {
@@ -795,13 +803,12 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
                                 }
                             });
                         }
-                        if (kPose) {
-                            mean64 = mean.value();
+                        words[0] = mean.sum;
+                        words[1] = mean.carry;
 #pragma unroll
-                            for (int k = 0; k < 3; ++k) {
-                                Gd[k] = G[k];
-                                Hd[k] = (double)Hs[k] / (double)S;
-                            }
+                        for (int k = 0; k < 3; ++k) {
+                            words[2 + k] = G[k];
+                            words[5 + k] = Hs[k];
                         }
                     } else {
                         // per-sample form (rays reaching 1e30 in grid coordinates)
@@ -874,16 +881,31 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C ? DPT_VJP_
                             }
                         }
                         if (kVol && pending >= 0) scatter_moments(pending, m);
-                        if (kPose) {
-                            mean64 = mean.value();
+                        words[0] = mean.sum;
+                        words[1] = mean.carry;
 #pragma unroll
-                            for (int k = 0; k < 3; ++k) {
-                                Gd[k] = G[k];
-                                Hd[k] = H[k];
-                            }
+                        for (int k = 0; k < 3; ++k) {
+                            words[2 + k] = G[k];
+                            words[5 + k] = H[k];
                         }
+                        words[8] = 1.0f;
                     }
                     if (kPose) {
+                        mean64 = (double)words[0] - (double)words[1];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            Gd[k] = words[2 + k];
+                            Hd[k] = words[8] != 0.0f ? (double)words[5 + k] : (double)words[5 + k] / (double)S;
+                        }
+                    }
+                    if constexpr (kMoments == kStoreMoments) {
+                        // the forward image of the compensated form, as the forward kernel forms it
+                        const float total = (float)(mean64 * (r.length * step));
+                        if (!isfinite(total)) bits |= 2;
+                        stored_image = total;
+#pragma unroll
+                        for (int k = 0; k < kMomentWords; ++k) stored[k] = words[k];
+                    } else if (kPose) {
                         const double* dr = r.direction;
                         const double g_along = fma(Gd[2], dr[2], fma(Gd[1], dr[1], Gd[0] * dr[0]));
                         const double h_along = fma(Hd[2], dr[2], fma(Hd[1], dr[1], Hd[0] * dr[0]));
@@ -1026,20 +1048,30 @@ cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packe
     return run(QuadF32{static_cast<const float4*>(packed), p.nx, p.ny, p.nz});
 }
 
-// Forward image plus the pose moments of every ray (FP32 arithmetic; see kStoreMoments).
+// Forward image plus the pose moments of every ray (FP32 or compensated arithmetic; see
+// kStoreMoments).
 cudaError_t launch_forward_moments(const dpt_problem& p, const RayArgs& a, const void* packed,
                                    float* image, float* moments, int64_t stride, cudaStream_t stream)
 {
     const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
     const MomentArgs ma{moments, stride, image};
-    if (p.layout == DPT_LAYOUT_DIRECT) {
-        PlainF32 f{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
-        k_vjp<DPT_ARITH_F32, PlainF32, false, true, float, kStoreMoments>
+    auto run = [&](auto arith, const auto& f) {
+        using FieldT = std::decay_t<decltype(f)>;
+        k_vjp<decltype(arith)::value, FieldT, false, true, float, kStoreMoments>
             <<<grid, kVjpBlock, 0, stream>>>(a, f, nullptr, 6, nullptr, nullptr, ma);
+    };
+    using F32 = std::integral_constant<int, DPT_ARITH_F32>;
+    using F32C = std::integral_constant<int, DPT_ARITH_F32C>;
+    const PlainF32 direct{static_cast<const float*>(packed), p.nx, p.ny, p.nz};
+    if (p.arith == DPT_ARITH_F32C) {
+        if (p.layout == DPT_LAYOUT_DIRECT)
+            run(F32C{}, direct);
+        else
+            run(F32C{}, PolyF32{static_cast<const float4*>(packed), p.nx, p.ny, p.nz});
+    } else if (p.layout == DPT_LAYOUT_DIRECT) {
+        run(F32{}, direct);
     } else {
-        QuadF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
-        k_vjp<DPT_ARITH_F32, QuadF32, false, true, float, kStoreMoments>
-            <<<grid, kVjpBlock, 0, stream>>>(a, f, nullptr, 6, nullptr, nullptr, ma);
+        run(F32{}, QuadF32{static_cast<const float4*>(packed), p.nx, p.ny, p.nz});
     }
     return cudaGetLastError();
 }
@@ -1053,12 +1085,20 @@ cudaError_t launch_pose_from_moments(const dpt_problem& p, const RayArgs& a, con
     const int mode = (flags & DPT_VJP_POSE12) ? 12 : ((flags & DPT_VJP_PER_RAY6) ? -6 : 6);
     const MomentArgs ma{const_cast<float*>(moments), stride, nullptr};
     const PlainF32 none{nullptr, p.nx, p.ny, p.nz};
-    if (p.image_dtype == DPT_F64)
-        k_vjp<DPT_ARITH_F32, PlainF32, false, true, double, kLoadMoments><<<grid, kVjpBlock, 0, stream>>>(
-            a, none, static_cast<const double*>(cotangent), mode, nullptr, partials, ma);
-    else
-        k_vjp<DPT_ARITH_F32, PlainF32, false, true, float, kLoadMoments><<<grid, kVjpBlock, 0, stream>>>(
-            a, none, static_cast<const float*>(cotangent), mode, nullptr, partials, ma);
+    auto run = [&](auto arith, const auto* seed) {
+        using SeedT = std::remove_cv_t<std::remove_pointer_t<decltype(seed)>>;
+        k_vjp<decltype(arith)::value, PlainF32, false, true, SeedT, kLoadMoments>
+            <<<grid, kVjpBlock, 0, stream>>>(a, none, seed, mode, nullptr, partials, ma);
+    };
+    using F32 = std::integral_constant<int, DPT_ARITH_F32>;
+    using F32C = std::integral_constant<int, DPT_ARITH_F32C>;
+    if (p.image_dtype == DPT_F64) {
+        const double* seed = static_cast<const double*>(cotangent);
+        if (p.arith == DPT_ARITH_F32C) run(F32C{}, seed); else run(F32{}, seed);
+    } else {
+        const float* seed = static_cast<const float*>(cotangent);
+        if (p.arith == DPT_ARITH_F32C) run(F32C{}, seed); else run(F32{}, seed);
+    }
     return cudaGetLastError();
 }
 

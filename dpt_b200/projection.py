@@ -441,9 +441,9 @@ class ProjectionWorkspace:
     MOMENT_BYTES_LIMIT = 16 << 30
 
     def moments_supported(self) -> bool:
-        """Whether a forward can store the pose moments for a later pose VJP (FP32 arithmetic
-        and images, within MOMENT_BYTES_LIMIT)."""
-        return (self.spec.arith == N.ARITH_F32 and self.spec.image_code == N.F32 and
+        """Whether a forward can store the pose moments for a later pose VJP (FP32 or
+        compensated arithmetic, FP32 images, within MOMENT_BYTES_LIMIT)."""
+        return (self.spec.arith in (N.ARITH_F32, N.ARITH_F32C) and self.spec.image_code == N.F32 and
                 N.library().dpt_b200_moments_bytes(self.problem, self.views) <= self.MOMENT_BYTES_LIMIT)
 
     def _moments_match(self, field: torch.Tensor, poses: torch.Tensor) -> bool:
@@ -461,7 +461,7 @@ class ProjectionWorkspace:
                 *, checked: bool = True, moments: bool = False) -> torch.Tensor:
         """Optical depth ``(views, rows, cols)`` (bundles: ``(rays,)``).
 
-        ``moments=True`` (FP32 arithmetic) also stores each ray's pose moments, so that a
+        ``moments=True`` (FP32 or compensated arithmetic) also stores each ray's pose moments, so that a
         following ``vjp`` with the same field and poses forms the pose gradient without
         sampling again; the image is identical either way."""
         with self.lock, torch.cuda.device(self.device):

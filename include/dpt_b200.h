@@ -196,9 +196,9 @@ int dpt_b200_vjp(const dpt_problem* problem, const dpt_rays* rays, const void* p
                  const void* cotangent, int32_t flags, float* accumulator,
                  double* pose_partials, int32_t* status, void* stream);
 
-/* Split pose VJP (DPT_ARITH_F32, FP32 images).  A ray's pose moments (its sample sum, sums of
- * the grid slopes and of the position-weighted slopes, and the two clip shifts: 9 FP32
- * words) do not depend on its cotangent.  dpt_b200_forward_moments writes the forward image
+/* Split pose VJP (DPT_ARITH_F32 or DPT_ARITH_F32C, FP32 images).  A ray's pose moments (its
+ * sample sum, sums of the grid slopes and of the position-weighted slopes, and for FP32 the
+ * two clip shifts: 9 FP32 words) do not depend on its cotangent.  dpt_b200_forward_moments writes the forward image
  * (identical to dpt_b200_forward) and stores the moments, word k of ray i of the call at
  * moments[k * view_count*rows*cols + i] (dpt_b200_moments_bytes);
  * dpt_b200_pose_from_moments then forms the pose partials of dpt_b200_vjp for one pose

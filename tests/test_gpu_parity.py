@@ -276,14 +276,16 @@ def test_signed_linear_domain_accepts_negative_fields():
 
 @pytest.mark.parametrize("pose_form", ["matrix", "tangent"])
 @pytest.mark.parametrize("volume", [True, False])
-def test_split_pose_vjp_from_forward_moments_equals_joint_vjp(pose_form, volume):
+@pytest.mark.parametrize("sampling,storage", [("float32", "float32"), ("compensated", "bfloat16")])
+def test_split_pose_vjp_from_forward_moments_equals_joint_vjp(pose_form, volume, sampling, storage):
     """A forward that stores the pose moments writes the same image, and the VJP that then
     forms the pose gradient from them (no second sampling pass) equals the joint VJP."""
     grid, geometry, values = cone_scene()
     poses = poses_for(len(geometry.views), seed=12)
-    field, pose = device_inputs(values, poses)
-    joint = workspace(grid, geometry, 53, widen=3)
-    split = workspace(grid, geometry, 53, widen=3)
+    dtype = torch.bfloat16 if storage == "bfloat16" else torch.float32
+    field, pose = device_inputs(values, poses, dtype)
+    joint = workspace(grid, geometry, 53, sampling, storage=storage, widen=3)
+    split = workspace(grid, geometry, 53, sampling, storage=storage, widen=3)
     image = joint.forward(field, pose)
     image_m = split.forward(field, pose, moments=True)
     torch.testing.assert_close(image_m, image, rtol=0, atol=0)
