@@ -15,7 +15,7 @@ from pathlib import Path
 from .contracts import ContractError
 
 LIBRARY_PATH = Path(__file__).resolve().parent / "_lib" / "libdpt_b200.so"
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # Mirrors of the header's enums.
 F32, F64, F16, BF16 = 0, 1, 2, 3
@@ -26,6 +26,10 @@ PANEL_CONE, PANEL_PARALLEL, PANEL_CURVED = 0, 1, 2
 VIEW_WORDS, VIEW_MODE_WORD = 20, 18
 LAYOUT_REPLICATED, LAYOUT_DIRECT = 0, 1
 VJP_VOLUME, VJP_POSE12, VJP_POSE6, VJP_PER_RAY6 = 1, 2, 4, 8
+OUT_TRANSMISSION, OUT_COUNTS, OUT_LOG_TRANSMISSION, OUT_REMOVED = 1, 2, 4, 8
+BEAM_NONE, BEAM_SCALAR, BEAM_DEVICE_SCALAR, BEAM_PER_PIXEL = 0, 1, 2, 3
+CHECK_FINITE_NONNEGATIVE, CHECK_FINITE, CHECK_DECREMENT = 0, 1, 2
+OBJECTIVE_SQUARED_ERROR, OBJECTIVE_POISSON = 0, 1
 
 EXPORTS = (
     "dpt_b200_abi_version",
@@ -43,6 +47,15 @@ EXPORTS = (
     "dpt_b200_moments_bytes",
     "dpt_b200_forward_moments",
     "dpt_b200_pose_from_moments",
+    "dpt_b200_reduction_bytes",
+    "dpt_b200_check_values",
+    "dpt_b200_transmit",
+    "dpt_b200_transmit_vjp",
+    "dpt_b200_depth_from_removed",
+    "dpt_b200_depth_from_removed_vjp",
+    "dpt_b200_objective_check",
+    "dpt_b200_objective",
+    "dpt_b200_reduce_sum",
 )
 
 
@@ -87,6 +100,9 @@ _P = ctypes.POINTER(Problem)
 _R = ctypes.POINTER(Rays)
 _V = ctypes.c_void_p
 _I = ctypes.c_int32
+_L = ctypes.c_int64
+_F = ctypes.c_float
+_D = ctypes.c_double
 
 _SIGNATURES = {
     "dpt_b200_abi_version": ([], ctypes.c_int),
@@ -104,6 +120,17 @@ _SIGNATURES = {
     "dpt_b200_moments_bytes": ([_P, _I], ctypes.c_size_t),
     "dpt_b200_forward_moments": ([_P, _R, _V, _V, _V, _V, _V], ctypes.c_int),
     "dpt_b200_pose_from_moments": ([_P, _R, _V, _V, _I, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_reduction_bytes": ([_L], ctypes.c_size_t),
+    "dpt_b200_check_values": ([_V, _L, _I, _V, _V], ctypes.c_int),
+    "dpt_b200_transmit": ([_V, _L, _I, _I, _V, _F, _V, _V, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_transmit_vjp": (
+        [_V, _L, _I, _V, _F, _V, _V, _V, _V, _V, _V, _V, _I, _V, _V], ctypes.c_int),
+    "dpt_b200_depth_from_removed": ([_V, _L, _V, _V], ctypes.c_int),
+    "dpt_b200_depth_from_removed_vjp": ([_V, _V, _L, _V, _I, _V, _V], ctypes.c_int),
+    "dpt_b200_objective_check": ([_V, _I, _V, _V, _V, _L, _I, _I, _V, _V], ctypes.c_int),
+    "dpt_b200_objective": (
+        [_V, _I, _I, _V, _V, _V, _L, _I, _D, _D, _V, _V, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_reduce_sum": ([_V, _L, _V, _V, _V, _V], ctypes.c_int),
 }
 
 _lock = threading.Lock()

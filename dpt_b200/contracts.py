@@ -10,6 +10,7 @@ domain raises ``TrialDomainError``.
 from __future__ import annotations
 
 import math
+import struct
 from numbers import Real
 from typing import Any
 
@@ -41,6 +42,18 @@ def finite_scalar(value: Any, name: str, *, minimum: float | None = None) -> flo
     if not math.isfinite(result) or (minimum is not None and result < minimum):
         qualifier = "finite" if minimum is None else f"finite and at least {minimum}"
         raise ContractError(f"{name} must be {qualifier}")
+    return result
+
+
+def binary32_scalar(value: Any, name: str, *, minimum: float | None = None) -> float:
+    """A finite real scalar rounded once to binary32; overflow to infinity is rejected."""
+    result = finite_scalar(value, name, minimum=minimum)
+    try:
+        result = struct.unpack("f", struct.pack("f", result))[0]
+    except (OverflowError, struct.error) as error:
+        raise ContractError(f"{name} cannot be represented in binary32") from error
+    if not math.isfinite(result):
+        raise ContractError(f"{name} cannot be represented in binary32")
     return result
 
 
@@ -79,12 +92,26 @@ PROJECTION_MESSAGES = {
 }
 
 
-def raise_device_status(code: int, operator: str, messages: dict[int, str] | None = None) -> None:
-    """Raise the typed error for a nonzero device status word; do nothing for zero."""
+def raise_device_status(
+    code: int,
+    operator: str,
+    messages: dict[int, str] | None = None,
+    *,
+    input_error: type[Exception] = ContractError,
+    range_error: type[Exception] = NumericalError,
+) -> None:
+    """Raise the typed error for a nonzero device status word; do nothing for zero.
+
+    Bit 1 raises ``input_error``, bit 8 ``TrialDomainError``, bit 2 ``range_error`` and
+    bit 4 ``NumericalError``, in that precedence (reference ``contracts.py:90-119``)."""
     if not code:
         return
     descriptions = PROJECTION_MESSAGES if messages is None else messages
     for bit, error_type in _STATUS_TYPES:
         if code & bit:
+            if bit == 1:
+                error_type = input_error
+            elif bit == 2:
+                error_type = range_error
             raise error_type(f"{operator}: {descriptions.get(bit, 'device error')}")
     raise NumericalError(f"{operator}: unknown device status {code}")

@@ -35,6 +35,17 @@
  *   dpt_b200_counts         <- per-ray clip interval of python/dpt/kernels/projection_fp32.py:78-109
  *                              and python/dpt/kernels/projection.py:147-184 (no separate
  *                              reference entry point; exported for bit-exact count checks)
+ *
+ * and, for the image-space steps either side of the projection (declared at the end):
+ *   dpt_b200_transmit       <- python/dpt/transmission.py:307-397 (transmit), kernels
+ *                              python/dpt/kernels/transmission.py:91-144
+ *   dpt_b200_transmit_vjp   <- python/dpt/transmission.py:480-605 (transmission_vjp), kernels
+ *                              python/dpt/kernels/transmission.py:146-268
+ *   dpt_b200_depth_from_removed(_vjp) <- python/dpt/transmission.py:607-730
+ *   dpt_b200_check_values   <- python/dpt/kernels/transmission.py:305-326 (input rules)
+ *   dpt_b200_objective(_check) <- python/dpt/objectives.py:189-305 (evaluate_objective),
+ *                              kernels python/dpt/kernels/objectives.py:23-211
+ *   dpt_b200_reduce_sum     <- python/dpt/objectives.py:414-450 (reduce_objective_components)
  */
 #ifndef DPT_B200_H
 #define DPT_B200_H
@@ -46,7 +57,7 @@
 extern "C" {
 #endif
 
-#define DPT_B200_ABI_VERSION 2
+#define DPT_B200_ABI_VERSION 3
 
 /* Storage / output element types. */
 enum {
@@ -249,6 +260,92 @@ int dpt_b200_counts(const dpt_problem* problem, const dpt_rays* rays, double* lo
 int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_rays* rays, const float* field,
                             const void* cotangent, int32_t components, double* pose_gradient,
                             int32_t* status, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Image-space transmission and objectives.  One thread per pixel; `count` pixels of
+ * contiguous device arrays, count <= 2^31 - 1.  FP64 local arithmetic rounded once into
+ * each destination.  Scalar results go through a fixed FP64 tree of 256-wide tiles in the
+ * caller's `scratch` (dpt_b200_reduction_bytes(count) bytes), so they are deterministic.
+ * Compute calls write no input-rule diagnostics: a checked caller runs the matching
+ * check call first, reads `status`, and only then computes.  Status bits (status[0]):
+ * 1 invalid input, 2 unrepresentable output or gradient, 8 Poisson prediction outside
+ * its trial domain.
+ * ------------------------------------------------------------------------------------- */
+
+/* Transmission outputs (mask bits) and open-beam forms. */
+enum {
+    DPT_OUT_TRANSMISSION = 1,      /* T = exp(-L) */
+    DPT_OUT_COUNTS = 2,            /* n0 T, formed from the FP64 factor */
+    DPT_OUT_LOG_TRANSMISSION = 4,  /* -L (IEEE negation) */
+    DPT_OUT_REMOVED = 8            /* 1 - T = -expm1(-L) */
+};
+enum {
+    DPT_BEAM_NONE = 0,
+    DPT_BEAM_SCALAR = 1,           /* host scalar `beam_scalar` */
+    DPT_BEAM_DEVICE_SCALAR = 2,    /* beam[0] */
+    DPT_BEAM_PER_PIXEL = 3         /* beam[p] */
+};
+/* Input rules of dpt_b200_check_values. */
+enum {
+    DPT_CHECK_FINITE_NONNEGATIVE = 0,
+    DPT_CHECK_FINITE = 1,
+    DPT_CHECK_DECREMENT = 2        /* finite, 0 <= v < 1 */
+};
+/* Objective kinds. */
+enum {
+    DPT_OBJECTIVE_SQUARED_ERROR = 0,  /* 0.5 (mu - y)^2 */
+    DPT_OBJECTIVE_POISSON = 1         /* half-deviance mu - y + y log(y / mu) */
+};
+
+/* FP64 scratch bytes of the reduction tree over `count` pixels (or `count` FP64 rows). */
+size_t dpt_b200_reduction_bytes(int64_t count);
+
+/* OR bit 1 into status[0] for any value that breaks `rule`. */
+int dpt_b200_check_values(const float* values, int64_t count, int32_t rule, int32_t* status,
+                          void* stream);
+
+/* Write the outputs selected by `mask` (each non-null when selected). */
+int dpt_b200_transmit(const float* depth, int64_t count, int32_t mask, int32_t beam_mode,
+                      const float* beam, float beam_scalar, float* transmission, float* counts,
+                      float* log_transmission, float* removed, void* stream);
+
+/* grad_depth = -T cT - n0 T cN - cLog + T cR (null cotangents are zero); grad_beam = T cN
+ * per pixel (DPT_BEAM_PER_PIXEL) or its fixed-order FP64 sum rounded into grad_beam[0]
+ * (DPT_BEAM_DEVICE_SCALAR, needs `scratch`).  At least one gradient; `accumulate` adds
+ * each destination before its single rounding. */
+int dpt_b200_transmit_vjp(const float* depth, int64_t count, int32_t beam_mode, const float* beam,
+                          float beam_scalar, const float* seed_transmission,
+                          const float* seed_counts, const float* seed_log_transmission,
+                          const float* seed_removed, float* grad_depth, float* grad_beam,
+                          double* scratch, int32_t accumulate, int32_t* status, void* stream);
+
+/* depth = -log1p(-removed) and its VJP grad = seed / (1 - removed). */
+int dpt_b200_depth_from_removed(const float* removed, int64_t count, float* depth, void* stream);
+int dpt_b200_depth_from_removed_vjp(const float* removed, const float* seed, int64_t count,
+                                    float* grad, int32_t accumulate, int32_t* status,
+                                    void* stream);
+
+/* Fixed-input rules (bit 1) for observation, weights (may be null) and valid (uint8 0/1, may
+ * be null) and, with a non-null prediction (DPT_F32 or DPT_F64), bit 2 for a non-finite
+ * prediction and bit 8 for a Poisson prediction < 0 or == 0 against a positive count. */
+int dpt_b200_objective_check(const void* prediction, int32_t prediction_dtype,
+                             const float* observation, const float* weights,
+                             const uint8_t* valid, int64_t count, int32_t kind,
+                             int32_t integer_counts, int32_t* status, void* stream);
+
+/* loss[0] = sum_p valid_p normalisation weights_p ell(prediction_p, observation_p) (FP64;
+ * null skips the loss) and seed_p = d/d prediction_p of that term times seed_scale, rounded
+ * once into the prediction's dtype (null skips the seed).  `wide` selects the FP64
+ * precision forms (required for DPT_F64; with DPT_F32 the FP32 prediction is widened). */
+int dpt_b200_objective(const void* prediction, int32_t prediction_dtype, int32_t wide,
+                       const float* observation, const float* weights, const uint8_t* valid,
+                       int64_t count, int32_t kind, double normalisation, double seed_scale,
+                       void* seed, double* scratch, double* loss, int32_t* status,
+                       void* stream);
+
+/* total[0] = fixed-order FP64 sum of `count` values (zero when empty). */
+int dpt_b200_reduce_sum(const double* values, int64_t count, double* scratch, double* total,
+                        int32_t* status, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,4 +1,5 @@
-"""Compile the CPU oracle (``projector_oracle.c``) into ``oracle/_build/liboracle.so``.
+"""Compile the CPU oracle (``projector_oracle.c``, ``pointwise_oracle.c``) into
+``oracle/_build/liboracle.so``.
 
 TEST INFRASTRUCTURE ONLY.  ``-ffp-contract=off`` keeps every fused multiply-add
 explicit so the oracle follows the same floating-point contract as the CUDA
@@ -14,7 +15,7 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SOURCE = HERE / "projector_oracle.c"
+SOURCES = (HERE / "projector_oracle.c", HERE / "pointwise_oracle.c")
 HEADER = HERE.parent / "include" / "dpt_b200.h"
 LIBRARY = HERE / "_build" / "liboracle.so"
 
@@ -24,7 +25,7 @@ def build(force: bool = False) -> Path:
     if (
         not force
         and LIBRARY.exists()
-        and LIBRARY.stat().st_mtime >= max(SOURCE.stat().st_mtime, HEADER.stat().st_mtime)
+        and LIBRARY.stat().st_mtime >= max(path.stat().st_mtime for path in (*SOURCES, HEADER))
     ):
         return LIBRARY
     compiler = shutil.which("gcc") or shutil.which("cc")
@@ -41,7 +42,7 @@ def build(force: bool = False) -> Path:
         "-fPIC",
         "-shared",
         "-std=c11",
-        str(SOURCE),
+        *(str(source) for source in SOURCES),
         "-o",
         str(LIBRARY),
         "-lm",
