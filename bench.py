@@ -58,7 +58,7 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--storage", choices=("float32", "bfloat16", "float16"), default="float32")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--seed", type=int, default=20261203)
-    parser.add_argument("--mode", choices=("iteration", "serving", "precision"), default="iteration",
+    parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise"), default="iteration",
                         help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
     parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
     parser.add_argument("--slots", type=int, default=4, help="serving mode: concurrent request streams")
@@ -679,6 +679,92 @@ def run_precision(args) -> None:
     print(json.dumps({"metric": "relative L2 vs FP64 on the stored values, S=1024", "results": report}), flush=True)
 
 
+def run_pointwise(args) -> None:
+    """HBM roofline of the image-space kernels on the full scan's image (views x detector^2
+    FP32 pixels, larger than L2): transmission forward (T; counts from a per-pixel beam), its
+    VJP, the inverse of the removed fraction, the input check and the fused Poisson
+    objective + seed.  Each op is launched unchecked back to back on one stream and timed
+    with CUDA events; achieved = algorithmic bytes (inputs read once, outputs written once)
+    / time.  The oracle's time on 2^22 pixels (one host thread) is printed beside it."""
+    import numpy as np
+    import torch
+
+    from dpt_b200 import _native as N
+    from dpt_b200.objectives import ObjectiveSpec, evaluate_objective, prepare_objective
+    from dpt_b200.transmission import (TransmissionSpec, optical_depth_from_removed, prepare_transmission,
+                                       transmission_vjp, transmit)
+
+    device = torch.device("cuda:0")
+    n = args.views * args.detector * args.detector
+    generator = torch.Generator(device=device).manual_seed(args.seed)
+    depth = torch.rand(n, device=device, generator=generator) * 6
+    beam = torch.rand(n, device=device, generator=generator) * 1000 + 10
+    seed = torch.rand(n, device=device, generator=generator) - 0.5
+    out = torch.empty(n, device=device)
+    grad = torch.empty(n, device=device)
+    removed = torch.rand(n, device=device, generator=generator) * 0.9
+    observation = torch.poisson(beam * torch.exp(-depth), generator=generator)
+    prediction = beam * torch.exp(-depth) + 0.5
+    loss = torch.empty(1, dtype=torch.float64, device=device)
+    plain = prepare_transmission(max_pixels=n, device=device)
+    counted = prepare_transmission(TransmissionSpec(beam="per-pixel"), max_pixels=n, device=device)
+    poisson = prepare_objective(ObjectiveSpec(kind="poisson", domain="counts"), max_pixels=n, device=device)
+    lib = N.library()
+    stream = torch.cuda.current_stream(device)
+    ops = [
+        ("transmit T", 8, lambda: transmit(depth, out_T=out, workspace=plain, validate=False)),
+        ("transmit counts (per-pixel beam)", 12,
+         lambda: transmit(depth, beam, out_counts=out, workspace=counted, validate=False)),
+        ("transmission VJP (T cotangent)", 12,
+         lambda: transmission_vjp(depth, cotangent_T=seed, out_grad_L=grad, workspace=plain, validate=False)),
+        ("optical depth from removed", 8,
+         lambda: optical_depth_from_removed(removed, out_L=out, workspace=plain, validate=False)),
+        ("input check (finite, nonnegative)", 4,
+         lambda: lib.dpt_b200_check_values(depth.data_ptr(), n, N.CHECK_FINITE_NONNEGATIVE, plain.status.ptr,
+                                           stream.cuda_stream)),
+        ("Poisson objective + seed", 12,
+         lambda: evaluate_objective(prediction, observation, out_loss=loss, out_cotangent=grad, workspace=poisson,
+                                    validate=False)),
+    ]
+    peak, peak_kind = measured_peak()
+    results = []
+    for name, bytes_per_pixel, op in ops:
+        for _ in range(max(3, args.warmup)):
+            op()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(args.steps):
+            op()
+        end.record(stream)
+        end.synchronize()
+        seconds = start.elapsed_time(end) * 1e-3 / args.steps
+        achieved = bytes_per_pixel * n / seconds / 1e9
+        results.append({"op": name, "pixels": n, "bytes_per_pixel": bytes_per_pixel,
+                        "us_per_launch": round(seconds * 1e6, 1), "achieved_gbs": round(achieved, 1),
+                        "frac_hbm": round(achieved / peak, 3)})
+    for ws in (plain, counted):
+        ws.consume_status()
+    poisson.consume_status()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import pointwise as P
+
+        sample = 1 << 22
+        d = depth[:sample].cpu().numpy()
+        started = time.perf_counter()
+        P.transmit(d)
+        P.objective(prediction[:sample].cpu().numpy(), observation[:sample].cpu().numpy(), poisson=True)
+        elapsed = time.perf_counter() - started
+        cpu = {"value": round(2 * sample / elapsed / 1e6, 1), "unit": "Mpixel-ops/s", "cores": 1, "kind": "port",
+               "sample": f"transmit (all four outputs) + Poisson objective on {sample} pixels"}
+    print(json.dumps({"metric": "image-space kernels, HBM roofline", "unit": "GB/s",
+                      "config": {"workload": f"{args.views} x {args.detector}^2 FP32 image ({n} pixels)",
+                                 "l2": "inputs larger than L2"},
+                      "peak": {"hbm_gbs": peak, "source": f"{peak_kind} MEASURED_PEAKS hbm_gbs"},
+                      "results": results, "cpu_baseline": cpu}), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -687,6 +773,8 @@ def main() -> None:
         run_serving(args)
     elif args.mode == "precision":
         run_precision(args)
+    elif args.mode == "pointwise":
+        run_pointwise(args)
     else:
         run_gpu(args)
 

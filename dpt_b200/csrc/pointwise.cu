@@ -2,12 +2,17 @@
 // Beer-Lambert transmission (reference python/dpt/kernels/transmission.py) and the fused
 // objective value and image-space seed (reference python/dpt/kernels/objectives.py:133-211).
 //
-// One thread per pixel.  Local arithmetic is FP64 and rounds once into each FP32 (or FP64)
-// destination, as the reference does.  Scalar results (an objective's loss, an active
-// shared beam's gradient) are reduced without floating-point atomics: the pixel kernel
-// writes one FP64 partial per 256-pixel tile, then a fixed tree of 256-wide tiles
-// (reference python/dpt/_reductions.py:27-63) reduces them and one thread rounds the total
-// into its destination, so every sum is deterministic for a given pixel count.
+// These kernels stream HBM: each thread owns U 16-byte vector groups of 4 pixels (group u
+// of thread t in block b starts at pixel 4 (256 (U b + u) + t)), issues every load before any
+// arithmetic so that enough bytes are in flight to cover DRAM latency, and falls back to
+// scalar accesses for a ragged tail or when a caller's pointer is not 16-byte aligned.
+// Local arithmetic is FP64 and rounds once into each FP32 (or FP64) destination, as the
+// reference does.  Scalar results (an objective's loss, an active shared beam's gradient)
+// are reduced without floating-point atomics: each thread sums its 4 U terms in (u, j)
+// order, the block sums its 256 threads pairwise into one FP64 partial per 1024 U pixels,
+// then a fixed tree of 256-wide tiles (reference python/dpt/_reductions.py:27-63) reduces
+// the partials and one thread rounds the total into its destination, so every sum is
+// deterministic for a given pixel count.
 //
 // Checks of fixed inputs (finite, nonnegative, inside a domain) are separate launches that
 // write nothing but the status word, so a checked host call can reject its inputs before any
@@ -15,18 +20,109 @@
 // Status bits: 1 invalid input, 2 an unrepresentable result, 8 a prediction outside the
 // Poisson trial domain.
 #include <cstdint>
+#include <initializer_list>
 
 #include "launch.h"
 
 namespace dpt {
 namespace {
 
-constexpr int kTile = 256;
+constexpr int kTile = 256;                           // threads per block
+constexpr int kVec = 4;                              // pixels per vector group
+// Vector groups per thread of each kernel: four (16 pixels) for the streaming kernels, fewer
+// where FP64 latency or register pressure wants more resident warps instead.
+constexpr int kStreamUnroll = 4;
+constexpr int kVjpUnroll = 2;
+constexpr int kObjectiveUnroll = 1;
 
 __device__ __forceinline__ void flag(int32_t* status, int bits)
 {
     if (bits) atomicOr(status, bits);
 }
+
+// First pixel of this thread's vector group u (U groups per thread).
+template <int U>
+__device__ __forceinline__ int64_t group_first(int u)
+{
+    return (((int64_t)blockIdx.x * U + u) * kTile + threadIdx.x) * kVec;
+}
+
+// Streaming loads and stores of one group: one 16-byte access when the group is whole and
+// the pointer aligned, else element by element (absent elements read as zero, not stored).
+__device__ __forceinline__ void load4(const float* __restrict__ ptr, int64_t p, int64_t count, bool vec, float* v)
+{
+    if (vec && p + kVec <= count) {
+        const float4 x = __ldcs(reinterpret_cast<const float4*>(ptr + p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) v[j] = p + j < count ? ptr[p + j] : 0.0f;
+    }
+}
+
+__device__ __forceinline__ void load4(const double* __restrict__ ptr, int64_t p, int64_t count, bool vec, double* v)
+{
+    if (vec && p + kVec <= count) {
+        const double2 a = __ldcs(reinterpret_cast<const double2*>(ptr + p));
+        const double2 b = __ldcs(reinterpret_cast<const double2*>(ptr + p + 2));
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) v[j] = p + j < count ? ptr[p + j] : 0.0;
+    }
+}
+
+__device__ __forceinline__ void load4(const uint8_t* __restrict__ ptr, int64_t p, int64_t count, bool vec, uint8_t* v)
+{
+    if (vec && p + kVec <= count) {
+        const uchar4 x = *reinterpret_cast<const uchar4*>(ptr + p);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) v[j] = p + j < count ? ptr[p + j] : 0;
+    }
+}
+
+__device__ __forceinline__ void store4(float* __restrict__ ptr, int64_t p, int64_t count, bool vec, const float* v)
+{
+    if (vec && p + kVec <= count) {
+        __stcs(reinterpret_cast<float4*>(ptr + p), make_float4(v[0], v[1], v[2], v[3]));
+    } else {
+#pragma unroll
+        for (int j = 0; j < kVec; ++j)
+            if (p + j < count) ptr[p + j] = v[j];
+    }
+}
+
+__device__ __forceinline__ void store4(double* __restrict__ ptr, int64_t p, int64_t count, bool vec, const double* v)
+{
+    if (vec && p + kVec <= count) {
+        __stcs(reinterpret_cast<double2*>(ptr + p), make_double2(v[0], v[1]));
+        __stcs(reinterpret_cast<double2*>(ptr + p + 2), make_double2(v[2], v[3]));
+    } else {
+#pragma unroll
+        for (int j = 0; j < kVec; ++j)
+            if (p + j < count) ptr[p + j] = v[j];
+    }
+}
+
+// The thread's kVec U pixels of `ptr` (group u, element j at index kVec u + j).
+template <int U, typename T>
+__device__ __forceinline__ void load_all(const T* __restrict__ ptr, int64_t count, bool vec, T* v)
+{
+#pragma unroll
+    for (int u = 0; u < U; ++u) load4(ptr, group_first<U>(u), count, vec, v + kVec * u);
+}
+
+template <int U, typename T>
+__device__ __forceinline__ void store_all(T* __restrict__ ptr, int64_t count, bool vec, const T* v)
+{
+#pragma unroll
+    for (int u = 0; u < U; ++u) store4(ptr, group_first<U>(u), count, vec, v + kVec * u);
+}
+
+template <int U>
+__device__ __forceinline__ int64_t pixel_at(int k) { return group_first<U>(k / kVec) + k % kVec; }
 
 // Fixed-order sum of one value per thread of a 256-thread block (pairwise tree in shared
 // memory); the total is valid in thread 0.
@@ -79,14 +175,19 @@ __device__ __forceinline__ float illumination(int beam_mode, const float* beam, 
 
 // Input rules of the reference's check kernels (kernels/transmission.py:305-326).
 __global__ void __launch_bounds__(kTile) k_check_values(const float* __restrict__ values, int64_t count,
-                                                        int rule, int32_t* status)
+                                                        int rule, int vec, int32_t* status)
 {
-    const int64_t p = (int64_t)blockIdx.x * kTile + threadIdx.x;
-    if (p >= count) return;
-    const float v = values[p];
-    bool bad = !isfinite(v);
-    if (rule != DPT_CHECK_FINITE) bad = bad || v < 0.0f;
-    if (rule == DPT_CHECK_DECREMENT) bad = bad || v >= 1.0f;
+    constexpr int U = kStreamUnroll, kPixels = kVec * U;
+    float v[kPixels];
+    load_all<U>(values, count, vec, v);
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < kPixels; ++k) {
+        bool b = !isfinite(v[k]);
+        if (rule != DPT_CHECK_FINITE) b = b || v[k] < 0.0f;
+        if (rule == DPT_CHECK_DECREMENT) b = b || v[k] >= 1.0f;
+        bad = bad || (b && pixel_at<U>(k) < count);
+    }
     if (bad) atomicOr(status, 1);
 }
 
@@ -96,25 +197,39 @@ __global__ void __launch_bounds__(kTile) k_transmit(const float* __restrict__ de
                                                     int beam_mode, const float* __restrict__ beam,
                                                     float beam_scalar, float* __restrict__ transmission,
                                                     float* __restrict__ counts, float* __restrict__ log_t,
-                                                    float* __restrict__ removed)
+                                                    float* __restrict__ removed, int vec)
 {
-    const int64_t p = (int64_t)blockIdx.x * kTile + threadIdx.x;
-    if (p >= count) return;
-    const float L = depth[p];
-    if (mask & (DPT_OUT_TRANSMISSION | DPT_OUT_COUNTS)) {
-        const double factor = transmission_factor(L);
-        if (mask & DPT_OUT_TRANSMISSION) transmission[p] = (float)factor;
-        if (mask & DPT_OUT_COUNTS) {
-            float c = (float)((double)illumination(beam_mode, beam, beam_scalar, p) * factor);
-            if (c == 0.0f) c = 0.0f;
-            counts[p] = c;
-        }
+    constexpr int U = kStreamUnroll, kPixels = kVec * U;
+    float L[kPixels], n0[kPixels], out[kPixels];
+    load_all<U>(depth, count, vec, L);
+    const bool per_pixel = (mask & DPT_OUT_COUNTS) && beam_mode == DPT_BEAM_PER_PIXEL;
+    if (per_pixel) load_all<U>(beam, count, vec, n0);
+    const float shared = beam_mode == DPT_BEAM_DEVICE_SCALAR && (mask & DPT_OUT_COUNTS) ? beam[0] : beam_scalar;
+    if (mask & DPT_OUT_TRANSMISSION) {
+#pragma unroll
+        for (int k = 0; k < kPixels; ++k) out[k] = (float)transmission_factor(L[k]);
+        store_all<U>(transmission, count, vec, out);
     }
-    if (mask & DPT_OUT_LOG_TRANSMISSION) log_t[p] = -L;
+    if (mask & DPT_OUT_COUNTS) {
+#pragma unroll
+        for (int k = 0; k < kPixels; ++k) {
+            const float c = (float)((double)(per_pixel ? n0[k] : shared) * transmission_factor(L[k]));
+            out[k] = c == 0.0f ? 0.0f : c;
+        }
+        store_all<U>(counts, count, vec, out);
+    }
+    if (mask & DPT_OUT_LOG_TRANSMISSION) {
+#pragma unroll
+        for (int k = 0; k < kPixels; ++k) out[k] = -L[k];
+        store_all<U>(log_t, count, vec, out);
+    }
     if (mask & DPT_OUT_REMOVED) {
-        float r = removed_primary(L);
-        if (r == 0.0f) r = 0.0f;
-        removed[p] = r;
+#pragma unroll
+        for (int k = 0; k < kPixels; ++k) {
+            const float r = removed_primary(L[k]);
+            out[k] = r == 0.0f ? 0.0f : r;
+        }
+        store_all<U>(removed, count, vec, out);
     }
 }
 
@@ -128,68 +243,105 @@ __device__ __forceinline__ float checked(double value, int& bits)
 
 // Pointwise VJP (reference get_vjp_kernel / weighted_depth_adjoint / get_beam_partial_kernel,
 // kernels/transmission.py:146-268): d/dL of sum cT T + cN n0 T - cLog L + cR (1 - T), the
-// per-pixel beam gradient cN T, and for a shared beam one FP64 partial of sum cN T per tile.
+// per-pixel beam gradient cN T, and for a shared beam one FP64 partial of sum cN T per block.
 // A missing cotangent is zero; `accumulate` adds the destination before the single rounding.
 __global__ void __launch_bounds__(kTile) k_transmit_vjp(
     const float* __restrict__ depth, int64_t count, int beam_mode, const float* __restrict__ beam,
     float beam_scalar, const float* __restrict__ seed_t, const float* __restrict__ seed_n,
     const float* __restrict__ seed_log, const float* __restrict__ seed_r, float* __restrict__ grad_depth,
-    float* __restrict__ grad_beam, double* __restrict__ beam_partials, int accumulate, int32_t* status)
+    float* __restrict__ grad_beam, double* __restrict__ beam_partials, int accumulate, int vec, int32_t* status)
 {
+    constexpr int U = kVjpUnroll, kPixels = kVec * U;
     __shared__ double tree[kTile];
-    const int64_t p = (int64_t)blockIdx.x * kTile + threadIdx.x;
-    double beam_term = 0.0;
+    float L[kPixels], a[kPixels], b[kPixels], c[kPixels], r[kPixels], n0[kPixels], out[kPixels];
+    load_all<U>(depth, count, vec, L);
+#pragma unroll
+    for (int k = 0; k < kPixels; ++k) a[k] = b[k] = c[k] = r[k] = 0.0f;
+    if (seed_t) load_all<U>(seed_t, count, vec, a);
+    if (seed_n) load_all<U>(seed_n, count, vec, b);
+    if (seed_log) load_all<U>(seed_log, count, vec, c);
+    if (seed_r) load_all<U>(seed_r, count, vec, r);
+    const bool per_pixel = seed_n && grad_depth && beam_mode == DPT_BEAM_PER_PIXEL;
+    if (per_pixel) load_all<U>(beam, count, vec, n0);
+    const float shared = seed_n && beam_mode == DPT_BEAM_DEVICE_SCALAR ? beam[0] : beam_scalar;
+    const bool exponential = seed_t || seed_n || seed_r;
     int bits = 0;
-    if (p < count) {
-        const float L = depth[p];
-        const double a = seed_t ? (double)seed_t[p] : 0.0;
-        const double b = seed_n ? (double)seed_n[p] : 0.0;
-        const double c = seed_log ? (double)seed_log[p] : 0.0;
-        const double r = seed_r ? (double)seed_r[p] : 0.0;
-        const double factor = (seed_t || seed_n || seed_r) ? transmission_factor(L) : 0.0;
-        if (grad_depth) {
-            const double n0 = seed_n ? (double)illumination(beam_mode, beam, beam_scalar, p) : 0.0;
-            const double optical = (r - a) * factor;
-            double derivative = fma(-(b * n0), factor, optical) - c;
-            if (accumulate) derivative += (double)grad_depth[p];
-            grad_depth[p] = checked(derivative, bits);
+    if (grad_depth) {
+        if (accumulate) load_all<U>(grad_depth, count, vec, out);
+#pragma unroll
+        for (int k = 0; k < kPixels; ++k) {
+            // absent cotangents enter as FP64 zeros without a conversion (the XU pipe that
+            // converts FP32 to FP64 bounds this kernel)
+            const double factor = exponential ? transmission_factor(L[k]) : 0.0;
+            const double ak = seed_t ? (double)a[k] : 0.0, bk = seed_n ? (double)b[k] : 0.0;
+            const double ck = seed_log ? (double)c[k] : 0.0, rk = seed_r ? (double)r[k] : 0.0;
+            const double beam_k = seed_n ? (double)(per_pixel ? n0[k] : shared) : 0.0;
+            const double optical = (rk - ak) * factor;
+            double derivative = fma(-(bk * beam_k), factor, optical) - ck;
+            if (accumulate) derivative += (double)out[k];
+            const float rounded = (float)derivative;
+            if (!isfinite(rounded) && pixel_at<U>(k) < count) bits |= 2;
+            out[k] = rounded;
         }
-        beam_term = b * factor;
-        if (grad_beam) {
-            double derivative = beam_term;
-            if (accumulate) derivative += (double)grad_beam[p];
-            grad_beam[p] = checked(derivative, bits);
+        store_all<U>(grad_depth, count, vec, out);
+    }
+    if (grad_beam) {
+        if (accumulate) load_all<U>(grad_beam, count, vec, out);
+#pragma unroll
+        for (int k = 0; k < kPixels; ++k) {
+            double derivative = (double)b[k] * (exponential ? transmission_factor(L[k]) : 0.0);
+            if (accumulate) derivative += (double)out[k];
+            const float rounded = (float)derivative;
+            if (!isfinite(rounded) && pixel_at<U>(k) < count) bits |= 2;
+            out[k] = rounded;
         }
+        store_all<U>(grad_beam, count, vec, out);
     }
     if (beam_partials) {
-        const double total = tile_sum(beam_term, tree);
+        double sum = 0.0;
+#pragma unroll
+        for (int k = 0; k < kPixels; ++k) sum += pixel_at<U>(k) < count ? (double)b[k] * transmission_factor(L[k]) : 0.0;
+        const double total = tile_sum(sum, tree);
         if (threadIdx.x == 0) beam_partials[blockIdx.x] = total;
     }
     flag(status, bits);
 }
 
 __global__ void __launch_bounds__(kTile) k_depth_from_removed(const float* __restrict__ decrement,
-                                                              int64_t count, float* __restrict__ depth)
+                                                              int64_t count, float* __restrict__ depth, int vec)
 {
-    const int64_t p = (int64_t)blockIdx.x * kTile + threadIdx.x;
-    if (p >= count) return;
-    float L = depth_from_decrement(decrement[p]);
-    if (L == 0.0f) L = 0.0f;
-    depth[p] = L;
+    constexpr int U = kStreamUnroll, kPixels = kVec * U;
+    float v[kPixels];
+    load_all<U>(decrement, count, vec, v);
+#pragma unroll
+    for (int k = 0; k < kPixels; ++k) {
+        const float L = depth_from_decrement(v[k]);
+        v[k] = L == 0.0f ? 0.0f : L;
+    }
+    store_all<U>(depth, count, vec, v);
 }
 
 // d/d delta of -log(1 - delta) is 1 / (1 - delta) (reference get_inverse_vjp_kernel).
 __global__ void __launch_bounds__(kTile) k_depth_from_removed_vjp(const float* __restrict__ decrement,
                                                                   const float* __restrict__ seed,
                                                                   int64_t count, float* __restrict__ grad,
-                                                                  int accumulate, int32_t* status)
+                                                                  int accumulate, int vec, int32_t* status)
 {
-    const int64_t p = (int64_t)blockIdx.x * kTile + threadIdx.x;
-    if (p >= count) return;
+    constexpr int U = kStreamUnroll, kPixels = kVec * U;
+    float d[kPixels], s[kPixels], out[kPixels];
+    load_all<U>(decrement, count, vec, d);
+    load_all<U>(seed, count, vec, s);
+    if (accumulate) load_all<U>(grad, count, vec, out);
     int bits = 0;
-    double derivative = (double)seed[p] / (1.0 - (double)decrement[p]);
-    if (accumulate) derivative += (double)grad[p];
-    grad[p] = checked(derivative, bits);
+#pragma unroll
+    for (int k = 0; k < kPixels; ++k) {
+        double derivative = (double)s[k] / (1.0 - (double)d[k]);
+        if (accumulate) derivative += (double)out[k];
+        const float rounded = (float)derivative;
+        if (!isfinite(rounded) && pixel_at<U>(k) < count) bits |= 2;
+        out[k] = rounded;
+    }
+    store_all<U>(grad, count, vec, out);
     flag(status, bits);
 }
 
@@ -221,30 +373,37 @@ __global__ void __launch_bounds__(kTile) k_objective_check(const T* __restrict__
                                                            const float* __restrict__ observation,
                                                            const float* __restrict__ weights,
                                                            const uint8_t* __restrict__ valid, int64_t count,
-                                                           int poisson, int integer_counts, int32_t* status)
+                                                           int poisson, int integer_counts, int vec, int32_t* status)
 {
-    const int64_t p = (int64_t)blockIdx.x * kTile + threadIdx.x;
-    if (p >= count) return;
+    constexpr int U = kStreamUnroll, kPixels = kVec * U;
+    T mu[kPixels];
+    float y[kPixels], w[kPixels];
+    uint8_t m[kPixels];
+    load_all<U>(observation, count, vec, y);
+    if (prediction) load_all<U>(prediction, count, vec, mu);
+    if (weights) load_all<U>(weights, count, vec, w);
+    if (valid) load_all<U>(valid, count, vec, m);
     int bits = 0;
-    bool active = true;
-    if (valid) {
-        if (valid[p] > 1) bits |= 1;
-        active = valid[p] == 1;
-    }
-    if (active) {
-        const float b = observation[p];
-        bool invalid = !isfinite(b);
-        if (poisson) {
-            invalid = invalid || b < 0.0f;
-            if (integer_counts) invalid = invalid || floorf(b) != b;
+#pragma unroll
+    for (int k = 0; k < kPixels; ++k) {
+        if (pixel_at<U>(k) >= count) continue;
+        bool active = true;
+        if (valid) {
+            if (m[k] > 1) bits |= 1;
+            active = m[k] == 1;
         }
-        if (weights) invalid = invalid || !isfinite(weights[p]) || weights[p] < 0.0f;
+        if (!active) continue;
+        bool invalid = !isfinite(y[k]);
+        if (poisson) {
+            invalid = invalid || y[k] < 0.0f;
+            if (integer_counts) invalid = invalid || floorf(y[k]) != y[k];
+        }
+        if (weights) invalid = invalid || !isfinite(w[k]) || w[k] < 0.0f;
         if (invalid) bits |= 1;
         if (prediction) {
-            const T a = prediction[p];
-            if (!isfinite(a))
+            if (!isfinite(mu[k]))
                 bits |= 2;
-            else if (poisson && (a < (T)0 || (a == (T)0 && b > 0.0f)))
+            else if (poisson && (mu[k] < (T)0 || (mu[k] == (T)0 && y[k] > 0.0f)))
                 bits |= 8;
         }
     }
@@ -253,7 +412,7 @@ __global__ void __launch_bounds__(kTile) k_objective_check(const T* __restrict__
 
 // Objective terms and the image-space seed (reference evaluation_kernel,
 // kernels/objectives.py:133-211).  kind: half squared error or Poisson half-deviance; each
-// active pixel's loss is weighted by normalisation x weights[p] and summed per tile into
+// active pixel's loss is weighted by normalisation x weights[p] and summed per block into
 // `partials` (skipped when null).  `kWide` selects the FP64-precision forms: the squared
 // loss as (0.5 w d) d and a Poisson seed recomputed as (w d) / mu when w / mu overflows.
 // The seed is (w x derivative) x seed_scale rounded once into TOut; seed_scale = 1 except
@@ -265,27 +424,33 @@ __global__ void __launch_bounds__(kTile) k_objective(const TIn* __restrict__ pre
                                                      const uint8_t* __restrict__ valid, int64_t count,
                                                      int poisson, double normalisation, double seed_scale,
                                                      TOut* __restrict__ seed, double* __restrict__ partials,
-                                                     int32_t* status)
+                                                     int vec, int32_t* status)
 {
+    constexpr int U = kObjectiveUnroll, kPixels = kVec * U;
     __shared__ double tree[kTile];
-    const int64_t p = (int64_t)blockIdx.x * kTile + threadIdx.x;
-    double loss = 0.0;
+    TIn mu[kPixels];
+    float y[kPixels], w[kPixels];
+    uint8_t m[kPixels];
+    TOut out[kPixels];
+    load_all<U>(prediction, count, vec, mu);
+    load_all<U>(observation, count, vec, y);
+    if (weights) load_all<U>(weights, count, vec, w);
+    if (valid) load_all<U>(valid, count, vec, m);
+    double sum = 0.0;
     int bits = 0;
-    if (p < count) {
-        bool active = true;
-        if (valid) {
-            if (valid[p] > 1) bits |= 1;
-            active = valid[p] == 1;
-        }
-        if (active) {
-            const double predicted = (double)prediction[p];
+#pragma unroll
+    for (int k = 0; k < kPixels; ++k) {
+        double loss = 0.0;
+        out[k] = (TOut)0.0;
+        if (pixel_at<U>(k) < count && (!valid || m[k] == 1)) {
+            const double predicted = (double)mu[k];
             if (!isfinite(predicted))
                 bits |= 2;
             else if (poisson && predicted < 0.0)
                 bits |= 8;
-            const double observed = (double)observation[p];
+            const double observed = (double)y[k];
             double weight = normalisation;
-            if (weights) weight *= (double)weights[p];
+            if (weights) weight *= (double)w[k];
             const double difference = predicted - observed;
             double derivative = difference;
             loss = 0.5 * difference * difference;
@@ -307,16 +472,16 @@ __global__ void __launch_bounds__(kTile) k_objective(const TIn* __restrict__ pre
             if (seed) {
                 double weighted = weight * derivative;
                 if (kWide && poisson && !isfinite(derivative)) weighted = (weight * difference) / predicted;
-                const TOut result = (TOut)(weighted * seed_scale);
-                seed[p] = result;
-                if (!isfinite((double)result)) bits |= 2;
+                out[k] = (TOut)(weighted * seed_scale);
+                if (!isfinite((double)out[k])) bits |= 2;
             }
-        } else if (seed) {
-            seed[p] = (TOut)0.0;
         }
+        if (valid && pixel_at<U>(k) < count && m[k] > 1) bits |= 1;
+        sum += loss;
     }
+    if (seed) store_all<U>(seed, count, vec, out);
     if (partials) {
-        const double total = tile_sum(loss, tree);
+        const double total = tile_sum(sum, tree);
         if (threadIdx.x == 0) partials[blockIdx.x] = total;
     }
     flag(status, bits);
@@ -347,6 +512,15 @@ __global__ void k_finish(const double* __restrict__ root, int nonempty, T* __res
 
 int64_t tiles(int64_t count) { return (count + kTile - 1) / kTile; }
 
+// Blocks of a pixel kernel with U groups per thread (1024 U pixels each): also its
+// first-level partial count.
+template <int U>
+int64_t blocks_for(int64_t count)
+{
+    constexpr int64_t pixels = (int64_t)kTile * kVec * U;
+    return (count + pixels - 1) / pixels;
+}
+
 // Rows of scratch the tree above `count` first-level rows needs (all levels after the first).
 int64_t tree_rows(int64_t count)
 {
@@ -375,6 +549,14 @@ void finish_tree(const double* first, int64_t count, double* scratch, T* destina
     k_finish<T><<<1, 1, 0, stream>>>(previous, nonempty, destination, accumulate, status);
 }
 
+// Vector accesses need every array 16-byte aligned (the uint8 mask 4-byte aligned).
+bool aligned(std::initializer_list<const void*> pointers, const void* mask = nullptr)
+{
+    for (const void* ptr : pointers)
+        if (ptr && reinterpret_cast<uintptr_t>(ptr) % 16) return false;
+    return !mask || reinterpret_cast<uintptr_t>(mask) % 4 == 0;
+}
+
 int launched() { return (int)cudaGetLastError(); }
 
 }  // namespace
@@ -387,6 +569,7 @@ extern "C" {
 size_t dpt_b200_reduction_bytes(int64_t count)
 {
     if (count < 0) return 0;
+    // covers both a pixel kernel's partials and its tree, and a tree over `count` rows
     const int64_t first = count ? dpt::tiles(count) : 0;
     return (size_t)(first + dpt::tree_rows(first) + 1) * sizeof(double);
 }
@@ -397,8 +580,8 @@ int dpt_b200_check_values(const float* values, int64_t count, int32_t rule, int3
     if (rule < DPT_CHECK_FINITE_NONNEGATIVE || rule > DPT_CHECK_DECREMENT) return DPT_E_FLAGS;
     if (!status || (count && !values)) return DPT_E_NULL;
     if (!count) return DPT_OK;
-    dpt::k_check_values<<<(unsigned)dpt::tiles(count), kTile, 0, static_cast<cudaStream_t>(stream)>>>(
-        values, count, rule, status);
+    dpt::k_check_values<<<(unsigned)dpt::blocks_for<dpt::kStreamUnroll>(count), kTile, 0, static_cast<cudaStream_t>(stream)>>>(
+        values, count, rule, dpt::aligned({values}), status);
     return dpt::launched();
 }
 
@@ -415,8 +598,10 @@ int dpt_b200_transmit(const float* depth, int64_t count, int32_t mask, int32_t b
         return DPT_E_NULL;
     if ((mask & DPT_OUT_COUNTS) && beam_mode >= DPT_BEAM_DEVICE_SCALAR && !beam) return DPT_E_NULL;
     if (!count) return DPT_OK;
-    dpt::k_transmit<<<(unsigned)dpt::tiles(count), kTile, 0, static_cast<cudaStream_t>(stream)>>>(
-        depth, count, mask, beam_mode, beam, beam_scalar, transmission, counts, log_transmission, removed);
+    const float* pixel_beam = (mask & DPT_OUT_COUNTS) && beam_mode == DPT_BEAM_PER_PIXEL ? beam : nullptr;
+    const bool vec = dpt::aligned({depth, pixel_beam, transmission, counts, log_transmission, removed});
+    dpt::k_transmit<<<(unsigned)dpt::blocks_for<dpt::kStreamUnroll>(count), kTile, 0, static_cast<cudaStream_t>(stream)>>>(
+        depth, count, mask, beam_mode, beam, beam_scalar, transmission, counts, log_transmission, removed, vec);
     return dpt::launched();
 }
 
@@ -439,13 +624,16 @@ int dpt_b200_transmit_vjp(const float* depth, int64_t count, int32_t beam_mode, 
     const bool per_pixel = grad_beam && beam_mode == DPT_BEAM_PER_PIXEL;
     const bool partials = shared && seed_counts && count;
     if (count && (grad_depth || per_pixel || partials)) {
-        dpt::k_transmit_vjp<<<(unsigned)dpt::tiles(count), kTile, 0, s>>>(
+        const float* pixel_beam = beam_mode == DPT_BEAM_PER_PIXEL ? beam : nullptr;
+        const bool vec = dpt::aligned({depth, pixel_beam, seed_transmission, seed_counts, seed_log_transmission,
+                                       seed_removed, grad_depth, per_pixel ? grad_beam : nullptr});
+        dpt::k_transmit_vjp<<<(unsigned)dpt::blocks_for<dpt::kVjpUnroll>(count), kTile, 0, s>>>(
             depth, count, beam_mode, beam, beam_scalar, seed_transmission, seed_counts, seed_log_transmission,
             seed_removed, grad_depth, per_pixel ? grad_beam : nullptr, partials ? scratch : nullptr, accumulate,
-            status);
+            vec, status);
     }
     if (shared) {
-        const int64_t rows = partials ? dpt::tiles(count) : 0;
+        const int64_t rows = partials ? dpt::blocks_for<dpt::kVjpUnroll>(count) : 0;
         dpt::finish_tree<float>(scratch, rows, scratch + rows, grad_beam, accumulate, status, s);
     }
     return dpt::launched();
@@ -456,8 +644,8 @@ int dpt_b200_depth_from_removed(const float* removed, int64_t count, float* dept
     if (count < 0 || count > INT32_MAX) return DPT_E_SHAPE;
     if (count && (!removed || !depth)) return DPT_E_NULL;
     if (!count) return DPT_OK;
-    dpt::k_depth_from_removed<<<(unsigned)dpt::tiles(count), kTile, 0, static_cast<cudaStream_t>(stream)>>>(
-        removed, count, depth);
+    dpt::k_depth_from_removed<<<(unsigned)dpt::blocks_for<dpt::kStreamUnroll>(count), kTile, 0, static_cast<cudaStream_t>(stream)>>>(
+        removed, count, depth, dpt::aligned({removed, depth}));
     return dpt::launched();
 }
 
@@ -467,8 +655,9 @@ int dpt_b200_depth_from_removed_vjp(const float* removed, const float* seed, int
     if (count < 0 || count > INT32_MAX) return DPT_E_SHAPE;
     if (!status || (count && (!removed || !seed || !grad))) return DPT_E_NULL;
     if (!count) return DPT_OK;
-    dpt::k_depth_from_removed_vjp<<<(unsigned)dpt::tiles(count), kTile, 0, static_cast<cudaStream_t>(stream)>>>(
-        removed, seed, count, grad, accumulate, status);
+    dpt::k_depth_from_removed_vjp<<<(unsigned)dpt::blocks_for<dpt::kStreamUnroll>(count), kTile, 0,
+                                    static_cast<cudaStream_t>(stream)>>>(
+        removed, seed, count, grad, accumulate, dpt::aligned({removed, seed, grad}), status);
     return dpt::launched();
 }
 
@@ -482,16 +671,17 @@ int dpt_b200_objective_check(const void* prediction, int32_t prediction_dtype, c
     if (!status || (count && !observation)) return DPT_E_NULL;
     if (!count) return DPT_OK;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const unsigned blocks = (unsigned)dpt::tiles(count);
+    const unsigned blocks = (unsigned)dpt::blocks_for<dpt::kStreamUnroll>(count);
     const int poisson = kind == DPT_OBJECTIVE_POISSON;
+    const bool vec = dpt::aligned({prediction, observation, weights}, valid);
     if (prediction_dtype == DPT_F64)
         dpt::k_objective_check<double><<<blocks, kTile, 0, s>>>(static_cast<const double*>(prediction),
                                                                 observation, weights, valid, count, poisson,
-                                                                integer_counts, status);
+                                                                integer_counts, vec, status);
     else
         dpt::k_objective_check<float><<<blocks, kTile, 0, s>>>(static_cast<const float*>(prediction),
                                                                observation, weights, valid, count, poisson,
-                                                               integer_counts, status);
+                                                               integer_counts, vec, status);
     return dpt::launched();
 }
 
@@ -509,25 +699,23 @@ int dpt_b200_objective(const void* prediction, int32_t prediction_dtype, int32_t
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int poisson = kind == DPT_OBJECTIVE_POISSON;
     double* partials = loss ? scratch : nullptr;
+    const int64_t blocks = dpt::blocks_for<dpt::kObjectiveUnroll>(count);
     if (count) {
-        const unsigned blocks = (unsigned)dpt::tiles(count);
+        const bool vec = dpt::aligned({prediction, observation, weights, seed}, valid);
         if (prediction_dtype == DPT_F64)
-            dpt::k_objective<double, double, true><<<blocks, kTile, 0, s>>>(
+            dpt::k_objective<double, double, true><<<(unsigned)blocks, kTile, 0, s>>>(
                 static_cast<const double*>(prediction), observation, weights, valid, count, poisson, normalisation,
-                seed_scale, static_cast<double*>(seed), partials, status);
+                seed_scale, static_cast<double*>(seed), partials, vec, status);
         else if (wide)
-            dpt::k_objective<float, float, true><<<blocks, kTile, 0, s>>>(
+            dpt::k_objective<float, float, true><<<(unsigned)blocks, kTile, 0, s>>>(
                 static_cast<const float*>(prediction), observation, weights, valid, count, poisson, normalisation,
-                seed_scale, static_cast<float*>(seed), partials, status);
+                seed_scale, static_cast<float*>(seed), partials, vec, status);
         else
-            dpt::k_objective<float, float, false><<<blocks, kTile, 0, s>>>(
+            dpt::k_objective<float, float, false><<<(unsigned)blocks, kTile, 0, s>>>(
                 static_cast<const float*>(prediction), observation, weights, valid, count, poisson, normalisation,
-                seed_scale, static_cast<float*>(seed), partials, status);
+                seed_scale, static_cast<float*>(seed), partials, vec, status);
     }
-    if (loss) {
-        const int64_t rows = dpt::tiles(count);
-        dpt::finish_tree<double>(scratch, rows, scratch + rows, loss, 0, status, s);
-    }
+    if (loss) dpt::finish_tree<double>(scratch, blocks, scratch + blocks, loss, 0, status, s);
     return dpt::launched();
 }
 

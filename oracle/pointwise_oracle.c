@@ -46,14 +46,34 @@ static double tree_sum(const double *rows, int64_t count)
     return total;
 }
 
-/* Per-pixel terms -> per-tile partials -> tree (the two stages the kernels run). */
-static double pixel_tree_sum(const double *terms, int64_t count)
+/* Per-pixel terms -> per-block partials -> tree (the two stages the kernels run).  With U
+ * vector groups per thread a block covers 1024 U pixels: thread t (0..255) sums, in (u, j)
+ * order, pixels 4 (256 (U b + u) + t) + j for u < U, j < 4 (absent pixels add zero); the
+ * block's 256 thread sums are then summed pairwise.  The shared-beam VJP runs with U = 2,
+ * the objective with U = 1. */
+#define VJP_UNROLL 2
+#define OBJECTIVE_UNROLL 1
+
+static double pixel_tree_sum(const double *terms, int64_t count, int unroll)
 {
     if (count <= 0) return 0.0;
-    const int64_t tiles = (count + TILE - 1) / TILE;
-    double *partials = malloc(sizeof(double) * (size_t)tiles);
-    for (int64_t b = 0; b < tiles; ++b) partials[b] = tile_sum(terms, b * TILE, count);
-    const double total = tree_sum(partials, tiles);
+    const int64_t block_pixels = (int64_t)TILE * 4 * unroll;
+    const int64_t blocks = (count + block_pixels - 1) / block_pixels;
+    double *partials = malloc(sizeof(double) * (size_t)blocks);
+    double threads[TILE];
+    for (int64_t b = 0; b < blocks; ++b) {
+        for (int t = 0; t < TILE; ++t) {
+            double sum = 0.0;
+            for (int u = 0; u < unroll; ++u)
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t p = ((b * unroll + u) * TILE + t) * 4 + j;
+                    sum += p < count ? terms[p] : 0.0;
+                }
+            threads[t] = sum;
+        }
+        partials[b] = tile_sum(threads, 0, TILE);
+    }
+    const double total = tree_sum(partials, blocks);
     free(partials);
     return total;
 }
@@ -157,7 +177,7 @@ int oracle_transmit_vjp(const float *depth, int64_t count, int beam_mode, const 
         if (terms) terms[p] = b * factor;
     }
     if (grad_beam_shared) {
-        grad_beam_shared[0] = (float)(seed_n ? pixel_tree_sum(terms, count) : 0.0);
+        grad_beam_shared[0] = (float)(seed_n ? pixel_tree_sum(terms, count, VJP_UNROLL) : 0.0);
         if (!isfinite(grad_beam_shared[0])) bits |= 2;
         free(terms);
     }
@@ -308,7 +328,7 @@ int oracle_objective(const void *prediction, int prediction_dtype, int wide, con
         }
     }
     if (loss) {
-        loss[0] = pixel_tree_sum(terms, count);
+        loss[0] = pixel_tree_sum(terms, count, OBJECTIVE_UNROLL);
         if (!isfinite(loss[0])) bits |= 2;
     }
     free(terms);

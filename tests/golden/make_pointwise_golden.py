@@ -93,8 +93,9 @@ def vjp_cases():
     rows = [rt.vjp_reference(float(depth[i]), float(beam[i]), seed_T=float(seeds["T"][i]),
                              seed_counts=float(seeds["counts"][i]), seed_log_T=float(seeds["log_T"][i]),
                              seed_removed=float(seeds["removed"][i])) for i in range(n)]
-    # the shared-beam sum in the kernels' order: 640 pixels -> 3 tiles of 256 -> one tile;
-    # each 256-wide tile is a depth-8 pairwise tree, so the longest path has 16 additions
+    # the shared-beam sum in the kernels' order: 640 pixels fall in one 2048-pixel block, whose
+    # threads add their (up to) 8 terms in sequence before a depth-8 pairwise tree over the
+    # 256 threads, so the longest path has 16 additions
     total, budget = rt.scalar_beam_reference(depth.tolist(), seeds["counts"].tolist(), addition_depth=16)
     return {
         "vjp_depth": depth,

@@ -383,3 +383,45 @@ def test_full_size_round_trip_and_determinism():
     evaluate_objective(prediction, observation, out_loss=first, workspace=objective_ws)
     evaluate_objective(prediction, observation, out_loss=second, workspace=objective_ws)
     assert float(first[0]) == float(second[0])
+
+
+@pytest.mark.parametrize("offset", [0, 1, 3])
+@pytest.mark.parametrize("size", [1, 5, 4095, 4097, 70003])
+def test_ragged_sizes_and_unaligned_views(offset, size):
+    """Tails that are not whole vector groups and views whose pointers are not 16-byte aligned
+    take the element-wise path and give the same bits as the aligned one."""
+    rng = np.random.default_rng(size + offset)
+    depth_np = rng.uniform(0, 5, size).astype(np.float32)
+    seed_np = rng.uniform(-1, 1, size).astype(np.float32)
+    storage = torch.zeros(size + 8, device=DEVICE)
+    storage[offset:offset + size] = dev(depth_np)
+    depth = storage[offset:offset + size]
+    outputs = torch.full((4, size + 8), 7.0, device=DEVICE)
+    views = [outputs[i, offset:offset + size] for i in range(4)]
+    ws = prepare_transmission(TransmissionSpec(beam="scalar"), max_pixels=size, device=DEVICE)
+    transmit(depth, 3.0, outputs=TransmissionOutputs(*views), workspace=ws)
+    aligned = [torch.empty(size, device=DEVICE) for _ in range(4)]
+    transmit(dev(depth_np), 3.0, outputs=TransmissionOutputs(*aligned), workspace=ws)
+    for view, reference in zip(views, aligned):
+        np.testing.assert_array_equal(host(view), host(reference))
+    assert (host(outputs[:, :offset]) == 7).all() and (host(outputs[:, offset + size:]) == 7).all()
+    grad_storage = torch.full((size + 8,), 5.0, device=DEVICE)
+    seed_storage = torch.zeros(size + 8, device=DEVICE)
+    seed_storage[offset:offset + size] = dev(seed_np)
+    transmission_vjp(depth, 3.0, cotangent_removed=seed_storage[offset:offset + size],
+                     out_grad_L=grad_storage[offset:offset + size], workspace=ws)
+    expected, _, _ = P.transmit_vjp(depth_np, seed_removed=seed_np)
+    assert ulps(host(grad_storage[offset:offset + size]), expected).max() <= 4
+    assert float(grad_storage[-1]) == 5.0
+    objective_ws = prepare_objective(ObjectiveSpec(weighted=True), max_pixels=size, device=DEVICE)
+    observation_np = rng.normal(size=size).astype(np.float32)
+    weights_np = rng.uniform(0, 1, size).astype(np.float32)
+    obs_storage = torch.zeros(size + 8, device=DEVICE)
+    obs_storage[offset:offset + size] = dev(observation_np)
+    loss = torch.empty(1, dtype=torch.float64, device=DEVICE)
+    cot = torch.empty(size + 8, device=DEVICE)
+    evaluate_objective(depth, obs_storage[offset:offset + size], out_loss=loss, out_cotangent=cot[offset:offset + size],
+                       weights=dev(weights_np), workspace=objective_ws)
+    oracle_loss, oracle_seed, _ = P.objective(depth_np, observation_np, weights=weights_np, poisson=False)
+    assert float(loss[0]) == oracle_loss
+    np.testing.assert_array_equal(host(cot[offset:offset + size]), oracle_seed)
