@@ -47,6 +47,10 @@ EXPORTS = (
     "dpt_b200_moments_bytes",
     "dpt_b200_forward_moments",
     "dpt_b200_pose_from_moments",
+    "dpt_b200_gather_plan_bytes",
+    "dpt_b200_gather_prepare",
+    "dpt_b200_gather_count",
+    "dpt_b200_gather",
     "dpt_b200_reduction_bytes",
     "dpt_b200_check_values",
     "dpt_b200_transmit",
@@ -120,6 +124,10 @@ _SIGNATURES = {
     "dpt_b200_moments_bytes": ([_P, _I], ctypes.c_size_t),
     "dpt_b200_forward_moments": ([_P, _R, _V, _V, _V, _V, _V], ctypes.c_int),
     "dpt_b200_pose_from_moments": ([_P, _R, _V, _V, _I, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_gather_plan_bytes": ([_P, _I], ctypes.c_size_t),
+    "dpt_b200_gather_prepare": ([_P, _R, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_gather_count": ([_P, _R, _V, _I, _V, _V], ctypes.c_int),
+    "dpt_b200_gather": ([_P, _R, _V, _V, _V, _I, _I, _V, _V], ctypes.c_int),
     "dpt_b200_reduction_bytes": ([_L], ctypes.c_size_t),
     "dpt_b200_check_values": ([_V, _L, _I, _V, _V], ctypes.c_int),
     "dpt_b200_transmit": ([_V, _L, _I, _I, _V, _F, _V, _V, _V, _V, _V], ctypes.c_int),

@@ -329,4 +329,85 @@ int dpt_b200_counts(const dpt_problem* p, const dpt_rays* r, double* lower, doub
     });
 }
 
+// ------------------------------------------------------------ deterministic adjoint gather
+
+namespace {
+
+int check_gather(const dpt_problem* p, const dpt_rays* r)
+{
+    int code = check_problem(p);
+    if (code != DPT_OK) return code;
+    if ((code = check_rays(p, r)) != DPT_OK) return code;
+    // the canonical weights of the gather are the strict FP64 midpoint forward's
+    if (p->arith != DPT_ARITH_F64) return DPT_E_DTYPE;
+    return DPT_OK;
+}
+
+dpt::GatherArgs gather_args(const dpt_problem& p, const dpt_rays& r, int32_t* status)
+{
+    dpt::GatherArgs a;
+    a.grid.nx = p.nx;
+    a.grid.ny = p.ny;
+    a.grid.nz = p.nz;
+    for (int k = 0; k < 9; ++k) a.grid.m[k] = p.object_to_grid[k];
+    for (int k = 0; k < 3; ++k) a.grid.g0[k] = p.grid_origin[k];
+    a.views = r.view_count;
+    a.view_begin = r.view_begin;
+    a.rows = p.rows;
+    a.cols = p.cols;
+    a.samples = p.samples;
+    a.ray_kind = p.ray_kind;
+    a.poses = r.poses;
+    a.view_table = r.view_table;
+    a.ray_sources = r.ray_sources;
+    a.ray_endpoints = r.ray_endpoints;
+    a.status = status;
+    return a;
+}
+
+}  // namespace
+
+size_t dpt_b200_gather_plan_bytes(const dpt_problem* p, int32_t view_count)
+{
+    if (check_problem(p) != DPT_OK || view_count < 1 || view_count > p->views) return 0;
+    const size_t words = (size_t)view_count * dpt::kGatherHeaderWords +
+                         (size_t)view_count * p->rows * p->cols * dpt::kGatherRayWords;
+    return words * sizeof(double);
+}
+
+int dpt_b200_gather_prepare(const dpt_problem* p, const dpt_rays* r, double* plan, int32_t* status, void* stream)
+{
+    int code = check_gather(p, r);
+    if (code != DPT_OK) return code;
+    if (!plan || !status) return DPT_E_NULL;
+    if (!aligned(plan, 8)) return DPT_E_ALIGN;
+    if (r->view_count > kMaxViewsPerLaunch) return DPT_E_SHAPE;
+    return to_code(dpt::launch_gather_prepare(gather_args(*p, *r, status), plan, static_cast<cudaStream_t>(stream)));
+}
+
+int dpt_b200_gather_count(const dpt_problem* p, const dpt_rays* r, const double* plan, int32_t max_rays_per_voxel,
+                          int64_t* totals, void* stream)
+{
+    int code = check_gather(p, r);
+    if (code != DPT_OK) return code;
+    if (!plan || !totals) return DPT_E_NULL;
+    if (max_rays_per_voxel < 1) return DPT_E_SHAPE;
+    if (!aligned(plan, 8) || !aligned(totals, 8)) return DPT_E_ALIGN;
+    return to_code(dpt::launch_gather_count(gather_args(*p, *r, nullptr), plan, max_rays_per_voxel,
+                                            reinterpret_cast<unsigned long long*>(totals),
+                                            static_cast<cudaStream_t>(stream)));
+}
+
+int dpt_b200_gather(const dpt_problem* p, const dpt_rays* r, const double* plan, const void* cotangent,
+                    void* gradient, int32_t gradient_dtype, int32_t accumulate, int32_t* status, void* stream)
+{
+    int code = check_gather(p, r);
+    if (code != DPT_OK) return code;
+    if (!plan || !cotangent || !gradient || !status) return DPT_E_NULL;
+    if (gradient_dtype != DPT_F32 && gradient_dtype != DPT_F64) return DPT_E_DTYPE;
+    if (!aligned(plan, 8)) return DPT_E_ALIGN;
+    return to_code(dpt::launch_gather(gather_args(*p, *r, status), plan, cotangent, p->image_dtype, gradient,
+                                      gradient_dtype, accumulate, static_cast<cudaStream_t>(stream)));
+}
+
 }  // extern "C"

@@ -83,6 +83,22 @@ __device__ __forceinline__ void matvec_t(const double* a, const double* v, doubl
         r[i] = fma(a[6 + i], v[2], fma(a[3 + i], v[1], a[i] * v[0]));
 }
 
+// Rigid pose: finite, R^T R = I within 1e-10, det(R) >= 0 (reference kernels/geometry.py:55-74).
+__device__ __forceinline__ bool rigid_pose(const double* p)
+{
+    bool valid = true;
+    for (int k = 0; k < 12; ++k) valid = valid && isfinite(p[k]);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double product = fma(p[6 + i], p[6 + j], fma(p[3 + i], p[3 + j], p[i] * p[j]));
+            if (fabs(product - (i == j ? 1.0 : 0.0)) > 1e-10) valid = false;
+        }
+    const double det = p[0] * (p[4] * p[8] - p[5] * p[7]) - p[1] * (p[3] * p[8] - p[5] * p[6]) +
+                       p[2] * (p[3] * p[7] - p[4] * p[6]);
+    if (det < 0.0) valid = false;
+    return valid;
+}
+
 // Ray index inside its view -> (pixel) for the tiled panel mapping, or the bundle index.
 // Returns false for padding threads.
 __device__ __forceinline__ bool ray_of_thread(const RayArgs& a, int tile, int* pixel)

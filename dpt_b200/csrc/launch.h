@@ -40,4 +40,32 @@ cudaError_t launch_fold(const dpt_problem& p, float* accumulator, double* total,
                         int accumulate_total, void* gradient, int gradient_dtype, int clear,
                         int32_t* status, cudaStream_t stream);
 
+// Deterministic adjoint gather (gather.cu).  Plan layout (FP64 words): per view a header of
+// kGatherHeaderWords (culling metrics, cone coefficients, cone flag), then per ray of every
+// view a record of kGatherRayWords.
+constexpr int kGatherHeaderWords = 32;
+constexpr int kGatherColumnError = 0, kGatherRowError = 1, kGatherPointError = 2, kGatherFallback = 5,
+              kGatherCoefficients = 6, kGatherCone = 18;
+constexpr int kGatherRayWords = 16;
+constexpr int kRayOrigin = 0, kRayDirection = 3, kRayLength = 6, kRayLower = 7, kRaySpan = 8, kRayStep = 9,
+              kRayError = 10;
+
+struct GatherArgs {
+    Grid grid;
+    int views;       // views of the plan (and of this call)
+    int view_begin;  // first absolute view
+    int rows, cols, samples, ray_kind;
+    const double* poses;       // absolute view indexing
+    const double* view_table;  // absolute view indexing
+    const double* ray_sources;
+    const double* ray_endpoints;
+    int32_t* status;           // absolute view indexing
+};
+
+cudaError_t launch_gather_prepare(const GatherArgs& a, double* plan, cudaStream_t stream);
+cudaError_t launch_gather_count(const GatherArgs& a, const double* plan, int max_rays, unsigned long long* totals,
+                                cudaStream_t stream);
+cudaError_t launch_gather(const GatherArgs& a, const double* plan, const void* cotangent, int seed_dtype,
+                          void* out, int out_dtype, int accumulate, cudaStream_t stream);
+
 }  // namespace dpt

@@ -22,22 +22,6 @@ __device__ __forceinline__ float bf16_bits_to_float(uint16_t b)
     return __uint_as_float((uint32_t)b << 16);
 }
 
-// Rigid pose: finite, R^T R = I within 1e-10, det(R) >= 0 (reference kernels/geometry.py:55-74).
-__device__ bool rigid_pose(const double* p)
-{
-    bool valid = true;
-    for (int k = 0; k < 12; ++k) valid = valid && isfinite(p[k]);
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) {
-            double product = fma(p[6 + i], p[6 + j], fma(p[3 + i], p[3 + j], p[i] * p[j]));
-            if (fabs(product - (i == j ? 1.0 : 0.0)) > 1e-10) valid = false;
-        }
-    const double det = p[0] * (p[4] * p[8] - p[5] * p[7]) - p[1] * (p[3] * p[8] - p[5] * p[6]) +
-                       p[2] * (p[3] * p[7] - p[4] * p[6]);
-    if (det < 0.0) valid = false;
-    return valid;
-}
-
 struct PackArgs {
     int nx, ny, nz;
     int signed_domain;  // DPT_DOMAIN_SIGNED: only non-finite values are flagged

@@ -637,3 +637,169 @@ def projection_pose_sensitivities(field: torch.Tensor, pose: torch.Tensor, *, co
                                   workspace: ProjectionWorkspace) -> torch.Tensor:
     """Per-ray weighted local-right pose Jacobian rows, shape (rays, 6)."""
     return workspace.pose_sensitivities(field, pose, cotangent)
+
+
+# ------------------------------------------------------------ deterministic adjoint gather
+
+def _gather_metadata(workspace: ProjectionWorkspace) -> tuple:
+    spec = workspace.spec
+    return (id(workspace.plan), spec.samples_per_ray, spec.sampling_precision, spec.integration, spec.precision)
+
+
+def _gather_problem(workspace: ProjectionWorkspace) -> N.Problem:
+    return workspace.plan.problem(workspace.spec.samples_per_ray, N.ARITH_F64, image_dtype=workspace.spec.image_code)
+
+
+@dataclass(frozen=True, eq=False)
+class PreparedProjectionAdjoint:
+    """Captured rays and culling metrics of the strict FP64 midpoint operator A(pose) of one
+    workspace (reference ``PreparedProjectionAdjoint``, python/dpt/projection.py:1087-1247).
+
+    The plan owns its FP64 ray records (independent of later changes to the pose buffer);
+    ``candidate_rays`` and ``quadrature_nodes`` count the (voxel, ray) and (voxel, sample)
+    pairs the culled gather visits, ``fallback_voxels`` the voxels whose detector bounds fell
+    back to the whole panel, ``device_bytes`` the plan's device memory."""
+
+    workspace: ProjectionWorkspace
+    records: torch.Tensor
+    poses: torch.Tensor
+    candidate_rays: int
+    quadrature_nodes: int
+    fallback_voxels: int
+    device_bytes: int
+    preparation_work_bound: int
+    metadata: tuple
+
+    @property
+    def work_bound(self) -> int:
+        return self.workspace.plan.grid.voxels + self.candidate_rays + self.quadrature_nodes
+
+
+def _write_gather_plan(workspace: ProjectionWorkspace, poses: torch.Tensor, nbytes: int) -> torch.Tensor:
+    lib = N.library()
+    problem = _gather_problem(workspace)
+    records = torch.empty(nbytes // 8, dtype=torch.float64, device=workspace.device)
+    rays = workspace.rays(poses)
+    workspace._run("gather_prepare", lambda: lib.dpt_b200_gather_prepare(
+        problem, rays, records.data_ptr(), workspace.status.data_ptr(), _stream(workspace.device)))
+    workspace.consume_status("prepared gather")
+    return records
+
+
+def prepare_projection_adjoint(pose: torch.Tensor, *, workspace: ProjectionWorkspace, max_work: int = 10_000_000,
+                               max_prepare_voxels: int = 16_777_216, max_rays_per_voxel: int = 256,
+                               max_bytes: int = 256 * 1024 * 1024) -> PreparedProjectionAdjoint:
+    """Capture the ray setup of A(pose) and its conservative strict-midpoint gather bounds.
+
+    Validates the poses (rigid) and every ray and sample node, then counts the candidate rays
+    and nodes of every voxel.  ``max_prepare_voxels`` and ``max_rays_per_voxel`` bound the
+    preparation and each voxel's candidate rectangle, ``max_work`` the all-node validation
+    and the plan's gather queries, ``max_bytes`` the plan's device memory."""
+    spec = workspace.spec
+    if spec.sampling_precision != "float64" or spec.integration != "midpoint":
+        raise ContractError("prepared gather requires strict float64 midpoint sampling")
+    for value, name in ((max_work, "max_work"), (max_prepare_voxels, "max_prepare_voxels"),
+                        (max_rays_per_voxel, "max_rays_per_voxel"), (max_bytes, "max_bytes")):
+        integer(value, name, minimum=1, maximum=2**63 - 1)
+    integer(max_rays_per_voxel, "max_rays_per_voxel", minimum=1, maximum=2**31 - 1)
+    voxels, pixels = workspace.plan.grid.voxels, workspace.plan.rays
+    setup_nodes = pixels * spec.samples_per_ray
+    if voxels > max_prepare_voxels or voxels > max_work:
+        raise ContractError("prepared gather exceeds max_prepare_voxels or max_work")
+    if setup_nodes > max_work:
+        raise ContractError("all-node ray validation exceeds max_work")
+    if voxels * pixels * (spec.samples_per_ray + 1) + voxels > 2**63 - 1:
+        raise ContractError("prepared gather work counters exceed signed 64-bit range")
+    lib = N.library()
+    problem = _gather_problem(workspace)
+    device_bytes = lib.dpt_b200_gather_plan_bytes(problem, workspace.views) + 12 * 8 * workspace.views + 32
+    if device_bytes > max_bytes:
+        raise ContractError(f"prepared gather requires {device_bytes} device bytes; max_bytes is {max_bytes}")
+    poses = workspace.check_poses(pose).clone()
+    records = _write_gather_plan(workspace, poses, device_bytes - 12 * 8 * workspace.views - 32)
+    totals = torch.zeros(4, dtype=torch.int64, device=workspace.device)
+    rays = workspace.rays(poses)
+    workspace._run("gather_count", lambda: lib.dpt_b200_gather_count(
+        problem, rays, records.data_ptr(), max_rays_per_voxel, totals.data_ptr(), _stream(workspace.device)))
+    candidate_rays, nodes, limited, fallbacks = (int(v) for v in totals.cpu().tolist())
+    if limited:
+        raise ContractError(f"{limited} voxel bounds exceed max_rays_per_voxel")
+    work = voxels + candidate_rays + nodes
+    if work > max_work:
+        raise ContractError(f"prepared gather needs {work} bounded queries; max_work is {max_work}")
+    return PreparedProjectionAdjoint(
+        workspace, records, poses, candidate_rays, nodes, fallbacks, device_bytes,
+        setup_nodes + pixels + voxels * min(pixels, max_rays_per_voxel), _gather_metadata(workspace))
+
+
+def projection_adjoint_gather(pose, *, cotangent: torch.Tensor, workspace: ProjectionWorkspace,
+                              out_mu: torch.Tensor | None = None,
+                              volume_gradient_precision: Literal["float32", "float64"] = "float64",
+                              accumulate: bool = False, validate: Literal["once", "always", "never"] | None = None,
+                              max_work: int = 10_000_000) -> torch.Tensor:
+    """``out_mu[v] = sum_p A(pose)[p, v] cotangent[p]``: the fixed-pose transpose of the strict
+    FP64 midpoint projection, gathered per voxel in a fixed order (views ascending, each
+    view's FP64 sum added to the running value; then rows, columns, samples ascending), so it
+    is bitwise reproducible (reference python/dpt/projection.py:1250-1405).
+
+    ``pose`` is a (views, 12) FP64 pose tensor or a ``PreparedProjectionAdjoint`` of this
+    workspace; ``cotangent`` has the image's shape and dtype; ``out_mu`` (voxels, FP64 by
+    default or FP32) is written, or added to with ``accumulate``, and returned.  A raw pose
+    bounds its all-ray work voxels x rays x samples by ``max_work`` before writing; a
+    prepared plan checks its retained bound."""
+    spec = workspace.spec
+    if spec.sampling_precision != "float64":
+        raise ContractError("deterministic gather requires strict float64 sampling")
+    if volume_gradient_precision not in ("float32", "float64"):
+        raise ContractError("volume_gradient_precision must be float32 or float64")
+    if type(accumulate) is not bool:
+        raise ContractError("accumulate must be a boolean")
+    integer(max_work, "max_work", minimum=1, maximum=2**63 - 1)
+    plan = pose if isinstance(pose, PreparedProjectionAdjoint) else None
+    if plan is not None and (plan.workspace is not workspace or plan.metadata != _gather_metadata(workspace)):
+        raise ContractError("prepared adjoint belongs to its original workspace configuration")
+    if plan is None and spec.integration != "midpoint":
+        raise ContractError("the deterministic gather integrates with midpoint samples")
+    voxels, pixels = workspace.plan.grid.voxels, workspace.plan.rays
+    work = plan.work_bound if plan is not None else voxels * pixels * spec.samples_per_ray
+    if work > max_work:
+        raise ContractError(f"deterministic gather needs at most {work} voxel/ray quadrature evaluations; "
+                            f"max_work is {max_work}")
+    flat = workspace._cotangent(cotangent)
+    dtype = torch.float64 if volume_gradient_precision == "float64" else torch.float32
+    if out_mu is None:
+        if accumulate:
+            raise ContractError("accumulate needs an out_mu to add to")
+        out_mu = torch.empty(workspace.plan.grid.shape, dtype=dtype, device=workspace.device)
+    if (not isinstance(out_mu, torch.Tensor) or out_mu.dtype != dtype or out_mu.device != workspace.device
+            or out_mu.numel() != voxels or not out_mu.is_contiguous()):
+        raise ContractError(f"out_mu must be a contiguous {dtype} tensor of {voxels} voxels on the workspace device")
+    reads = [("cotangent", flat)]
+    if plan is not None:
+        reads.append(("prepared metrics", plan.records))
+    for name, tensor in reads:
+        a0, a1 = out_mu.data_ptr(), out_mu.data_ptr() + out_mu.numel() * out_mu.element_size()
+        b0, b1 = tensor.data_ptr(), tensor.data_ptr() + tensor.numel() * tensor.element_size()
+        if a0 < b1 and b0 < a1:
+            raise ContractError(f"out_mu overlaps {name}")
+    policy = spec.validate if validate is None else validate
+    if policy not in ("once", "always", "never"):
+        raise ContractError("validate must be once, always or never")
+    if policy != "never" and not bool(torch.isfinite(flat).all()):
+        raise NumericalError("projection: the cotangent must be finite")
+    if plan is not None:
+        records, poses = plan.records, plan.poses
+    else:
+        poses = workspace.check_poses(pose)
+        nbytes = N.library().dpt_b200_gather_plan_bytes(_gather_problem(workspace), workspace.views)
+        records = _write_gather_plan(workspace, poses, nbytes)
+    lib = N.library()
+    problem = _gather_problem(workspace)
+    rays = workspace.rays(poses)
+    code = N.F64 if dtype == torch.float64 else N.F32
+    workspace._run("gather", lambda: lib.dpt_b200_gather(
+        problem, rays, records.data_ptr(), flat.data_ptr(), out_mu.data_ptr(), code, int(accumulate),
+        workspace.status.data_ptr(), _stream(workspace.device)))
+    if policy != "never":
+        workspace.consume_status("deterministic gather")
+    return out_mu

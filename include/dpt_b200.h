@@ -35,6 +35,11 @@
  *   dpt_b200_counts         <- per-ray clip interval of python/dpt/kernels/projection_fp32.py:78-109
  *                              and python/dpt/kernels/projection.py:147-184 (no separate
  *                              reference entry point; exported for bit-exact count checks)
+ *   dpt_b200_gather_prepare <- python/dpt/projection.py:1087-1247 (prepare_projection_adjoint),
+ *                              kernels python/dpt/kernels/projection_adjoint.py:184-368
+ *   dpt_b200_gather_count   <- python/dpt/kernels/projection_adjoint.py:371-581 (bounds, work count)
+ *   dpt_b200_gather         <- python/dpt/projection.py:1250-1405 (projection_adjoint_gather),
+ *                              kernels python/dpt/kernels/projection_adjoint.py:34-170, 583-635
  *
  * and, for the image-space steps either side of the projection (declared at the end):
  *   dpt_b200_transmit       <- python/dpt/transmission.py:307-397 (transmit), kernels
@@ -260,6 +265,35 @@ int dpt_b200_counts(const dpt_problem* problem, const dpt_rays* rays, double* lo
 int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_rays* rays, const float* field,
                             const void* cotangent, int32_t components, double* pose_gradient,
                             int32_t* status, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Deterministic adjoint gather: out[v] = sum_p A[p, v] cotangent[p] for the strict FP64
+ * midpoint projection (arith DPT_ARITH_F64), one thread per voxel summing in FP64 in a fixed
+ * order (views ascending, each view's sum added to the running value; then detector rows,
+ * columns and samples ascending), so the result is bitwise reproducible.  A plan holds the
+ * rays of views [view_begin, view_begin + view_count) of `rays` and their culling metrics;
+ * the culled sum is bitwise equal to the sum over all rays and samples.
+ * ------------------------------------------------------------------------------------- */
+
+/* Bytes of a plan for `view_count` views (32 + 16 x rays per view doubles per view). */
+size_t dpt_b200_gather_plan_bytes(const dpt_problem* problem, int32_t view_count);
+
+/* Write the plan: ray records, point-rounding bounds, cone culling metrics.  Invalid rays and
+ * non-finite sample points set bit 2 in their view's status word (the plan is then unusable). */
+int dpt_b200_gather_prepare(const dpt_problem* problem, const dpt_rays* rays, double* plan,
+                            int32_t* status, void* stream);
+
+/* totals[0..3] = candidate rays, sample nodes, voxels over `max_rays_per_voxel` candidate rays
+ * in some view, voxels whose culling fell back to the whole panel (summed over views). */
+int dpt_b200_gather_count(const dpt_problem* problem, const dpt_rays* rays, const double* plan,
+                          int32_t max_rays_per_voxel, int64_t* totals, void* stream);
+
+/* gradient (voxels, DPT_F32 or DPT_F64) = (accumulate ? gradient : 0) + gather of the
+ * cotangent (view_count x rows x cols, problem->image_dtype); a non-finite result sets bit 2
+ * in status[view_begin]. */
+int dpt_b200_gather(const dpt_problem* problem, const dpt_rays* rays, const double* plan,
+                    const void* cotangent, void* gradient, int32_t gradient_dtype,
+                    int32_t accumulate, int32_t* status, void* stream);
 
 /* ---------------------------------------------------------------------------------------
  * Image-space transmission and objectives.  One thread per pixel; `count` pixels of

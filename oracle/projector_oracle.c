@@ -1935,3 +1935,92 @@ int oracle_check_pose(const double* pose)
 }
 
 int oracle_abi_version(void) { return DPT_B200_ABI_VERSION; }
+
+/* ---------------------------------------------------- deterministic adjoint gather */
+
+/* a b c d with the mantissas multiplied in [2^-4, 1) and the exponents added, one final
+ * scaling (numerics.py product4, :11-62) */
+static double range_product4(double a, double b, double c, double d)
+{
+    if (!isfinite(a) || !isfinite(b) || !isfinite(c) || !isfinite(d)) return a * b * c * d;
+    if (a == 0.0 || b == 0.0 || c == 0.0 || d == 0.0) return 0.0;
+    int ea, eb, ec, ed;
+    double ma = frexp(a, &ea), mb = frexp(b, &eb), mc = frexp(c, &ec), md = frexp(d, &ed);
+    return ldexp(ma * mb * mc * md, ea + eb + ec + ed);
+}
+
+/* point_contribution (projection_adjoint.py:34-45): the corner terms of sample q that land on
+ * `voxel`, in corner order, each scaled_corner_weight */
+static double point_contribution(int64_t voxel, const double* q, const int* shape, double seed)
+{
+    double result = 0.0;
+    if (!inside64(q, shape)) return result;
+    int lower[3];
+    double fraction[3];
+    cell_lower64(q, shape, lower);
+    fraction64(q, lower, shape, fraction);
+    for (int c = 0; c < 8; ++c)
+        if (corner_index(lower, shape, c) == voxel) result += scaled_corner64(fraction, c, seed);
+    return result;
+}
+
+/* get_gather (projection_adjoint.py:73-170), midpoint: every view's sum over all of its rays
+ * and samples, formed from zero per view and added to the running value (a per-view loop
+ * with accumulation), FP64 or FP32 output.  cotangent has the image dtype. */
+int oracle_gather(const dpt_problem* p, const double* poses, const double* view_table,
+                  const double* sources, const double* endpoints, const void* cotangent, void* out,
+                  int out_dtype, int accumulate, int32_t* status, int threads)
+{
+    const int shape[3] = {p->nx, p->ny, p->nz}, S = p->samples;
+    const int64_t voxels = (int64_t)p->nx * p->ny * p->nz, per_view = (int64_t)p->rows * p->cols;
+    int bits = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bits)
+#endif
+    for (int64_t voxel = 0; voxel < voxels; ++voxel) {
+        double value = 0.0;
+        int running = accumulate;
+        if (accumulate) value = out_dtype == DPT_F64 ? ((double*)out)[voxel] : (double)((float*)out)[voxel];
+        for (int view = 0; view < p->views; ++view) {
+            double total = 0.0;
+            for (int64_t pixel = 0; pixel < per_view; ++pixel) {
+                double source[3], end[3];
+                ray_t ray;
+                ray_endpoints(p, view_table, sources, endpoints, view, pixel, source, end);
+                ray_setup(p, poses + 12 * view, source, end, &ray.r);
+                if (!valid_ray(&ray.r)) {
+                    bits |= 2;
+                    continue;
+                }
+                const double seed = (double)load_image(p, cotangent, (int64_t)view * per_view + pixel);
+                if (seed == 0.0) continue;
+                clip64(ray.r.origin, ray.r.direction, shape, &ray.iv64);
+                const double span = ray.iv64.upper - ray.iv64.lower;
+                if (span <= 0.0) continue;
+                const double factor = seed * ray.r.length;
+                const double step = span / (double)S;
+                double scale = factor * span / (double)S;
+                if (!isfinite(factor)) scale = range_product4(seed, ray.r.length, span, 1.0 / (double)S);
+                for (int i = 0; i < S; ++i) {
+                    double position = fma((double)i + 0.5, step, ray.iv64.lower), q[3];
+                    for (int a = 0; a < 3; ++a) q[a] = fma(position, ray.r.direction[a], ray.r.origin[a]);
+                    if (!finite3(q)) bits |= 2;
+                    total += point_contribution(voxel, q, shape, scale);
+                }
+            }
+            if (out_dtype == DPT_F64)
+                value = running ? total + value : total;
+            else
+                value = (double)(float)(running ? total + value : total);
+            running = 1;
+        }
+        if (out_dtype == DPT_F64)
+            ((double*)out)[voxel] = value;
+        else
+            ((float*)out)[voxel] = (float)value;
+        if (!isfinite(value)) bits |= 2;
+    }
+    status[0] |= bits;
+    return 0;
+}

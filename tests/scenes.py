@@ -107,3 +107,19 @@ def poses_for(views: int, seed: int = 1, scale: float = 0.05) -> np.ndarray:
 
 def identity_poses(views: int) -> np.ndarray:
     return np.tile(np.asarray(RigidTransform().packed()), (views, 1))
+
+
+def gather_scene(name: str):
+    """(grid, geometry, packed pose, samples) of a deterministic-gather golden scene."""
+    record = json.loads((GOLDEN / "gather.json").read_text())[name]
+    geometry = record["geometry"]
+    if geometry["kind"] == "bundle":
+        panel = RayBundleGeometry(tuple(tuple(s) for s in geometry["sources_mm"]),
+                                  tuple(tuple(e) for e in geometry["endpoints_mm"]))
+    else:
+        panel = panel_from(geometry)
+    return grid_from(record["grid"]), panel, np.asarray(record["pose"], dtype=np.float64), record["samples"]
+
+
+def gather_matrix(name: str) -> np.ndarray:
+    return np.load(GOLDEN / "gather.npz")[f"{name}_matrix"]
