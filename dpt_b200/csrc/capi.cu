@@ -338,8 +338,8 @@ int check_gather(const dpt_problem* p, const dpt_rays* r)
     int code = check_problem(p);
     if (code != DPT_OK) return code;
     if ((code = check_rays(p, r)) != DPT_OK) return code;
-    // the canonical weights of the gather are the strict FP64 midpoint forward's
-    if (p->arith != DPT_ARITH_F64) return DPT_E_DTYPE;
+    // the canonical weights of the gather are the strict FP64 forward's (midpoint or cell-Gauss)
+    if (p->arith != DPT_ARITH_F64 && p->arith != DPT_ARITH_CELLS) return DPT_E_DTYPE;
     return DPT_OK;
 }
 
@@ -357,6 +357,7 @@ dpt::GatherArgs gather_args(const dpt_problem& p, const dpt_rays& r, int32_t* st
     a.cols = p.cols;
     a.samples = p.samples;
     a.ray_kind = p.ray_kind;
+    a.cells = p.arith == DPT_ARITH_CELLS;
     a.poses = r.poses;
     a.view_table = r.view_table;
     a.ray_sources = r.ray_sources;
@@ -391,6 +392,7 @@ int dpt_b200_gather_count(const dpt_problem* p, const dpt_rays* r, const double*
     int code = check_gather(p, r);
     if (code != DPT_OK) return code;
     if (!plan || !totals) return DPT_E_NULL;
+    if (p->arith != DPT_ARITH_F64) return DPT_E_DTYPE;  // sample culling is for midpoint plans
     if (max_rays_per_voxel < 1) return DPT_E_SHAPE;
     if (!aligned(plan, 8) || !aligned(totals, 8)) return DPT_E_ALIGN;
     return to_code(dpt::launch_gather_count(gather_args(*p, *r, nullptr), plan, max_rays_per_voxel,

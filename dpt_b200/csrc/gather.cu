@@ -1,5 +1,6 @@
-// gather.cu - deterministic voxel-driven transpose of the strict FP64 midpoint projection
-// (reference python/dpt/projection.py:1087-1405, kernels python/dpt/kernels/projection_adjoint.py).
+// gather.cu - deterministic voxel-driven transpose of the strict FP64 projection, midpoint or
+// cell-Gauss (reference python/dpt/projection.py:1087-1405, kernels
+// python/dpt/kernels/projection_adjoint.py).
 //
 // out[v] = sum over views, rays p and midpoint samples s of the corner weight of voxel v at
 // sample s of ray p, times cotangent[p] |e - s| span / S, summed per voxel in FP64 in a fixed
@@ -180,9 +181,34 @@ __global__ void __launch_bounds__(256) k_gather_rays(GatherArgs a, double* __res
     rec[kRayLower] = iv.lower;
     rec[kRaySpan] = span;
     rec[kRayStep] = step;
+    rec[kRayUpper] = iv.upper;
+    if (a.cells && bits == 0 && iv.upper - iv.lower > 0.0) {
+        // every segment of the cell walk must advance and have finite Gauss nodes (reference
+        // get_gather cell_gauss, projection_adjoint.py:105-146); checked once per ray here
+        const int shape[3] = {a.grid.nx, a.grid.ny, a.grid.nz};
+        FieldDims dims;
+        dims.init(a.grid);
+        CellWalk64 walk;
+        walk.begin(r, iv.lower, iv.upper, shape);
+        double start = iv.lower;
+        const int64_t limit = (int64_t)shape[0] + shape[1] + shape[2] + 1;
+        for (int64_t n = 0; start < iv.upper && n < limit; ++n) {
+            GaussSegment seg;
+            walk.segment(r, start, dims, seg);
+            if (seg.end <= start) {
+                bits |= 2;
+                break;
+            }
+            if (!finite3(seg.first[0], seg.first[1], seg.first[2]) || !finite3(seg.second[0], seg.second[1], seg.second[2]))
+                bits |= 2;
+            start = seg.end;
+            walk.advance(r, shape, seg.end, iv.upper);
+        }
+        if (start < iv.upper) bits |= 2;
+    }
     // every sample point is finite when |origin| and |direction| are moderate (points are
     // o + t d with t in [0, 1]); otherwise check them all
-    if (span > 0.0 && !moderate(r.origin, r.direction)) {
+    if (!a.cells && span > 0.0 && !moderate(r.origin, r.direction)) {
         for (int i = 0; i < a.samples; ++i) {
             const double position = fma((double)i + 0.5, step, iv.lower);
             if (!finite3(fma(position, r.direction[0], r.origin[0]), fma(position, r.direction[1], r.origin[1]),
@@ -424,6 +450,122 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(GatherArgs a, const d
     if (!isfinite((double)value)) atomicOr(a.status + a.view_begin, 2);
 }
 
+// a b c without premature overflow or underflow of the partial products (reference numerics
+// product3).
+__device__ __forceinline__ double range_product(double a, double b, double c)
+{
+    if (!isfinite(a) || !isfinite(b) || !isfinite(c)) return a * b * c;
+    if (a == 0.0 || b == 0.0 || c == 0.0) return 0.0;
+    int ea, eb, ec;
+    const double ma = frexp(a, &ea), mb = frexp(b, &eb), mc = frexp(c, &ec);
+    return ldexp(ma * mb * mc, ea + eb + ec);
+}
+
+// Both Gauss nodes of a segment whose nodes share its interpolation cell (reference
+// cell_contribution): per corner of that cell landing on the voxel, first + second, a node
+// outside the support weighted by zero.
+__device__ __forceinline__ double cell_terms(const GaussSegment& s, const int* shape, const int* voxel, double seed)
+{
+    unsigned match[3];
+    double f1[3], f2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        match[k] = (min(s.lower[k], shape[k] - 1) == voxel[k] ? 1u : 0u) |
+                   (min(s.lower[k] + 1, shape[k] - 1) == voxel[k] ? 2u : 0u);
+        const double high = (double)(shape[k] - 1);
+        f1[k] = fmin(fmax(s.first[k], 0.0), high) - (double)s.lower[k];
+        f2[k] = fmin(fmax(s.second[k], 0.0), high) - (double)s.lower[k];
+    }
+    double result = 0.0;
+    if (!(match[0] && match[1] && match[2])) return result;
+    const double a = inside(s.first[0], s.first[1], s.first[2], shape[0], shape[1], shape[2]) ? seed : 0.0;
+    const double b = inside(s.second[0], s.second[1], s.second[2], shape[0], shape[1], shape[2]) ? seed : 0.0;
+#pragma unroll
+    for (int corner = 0; corner < 8; ++corner) {
+        const int bx = corner & 1, by = (corner >> 1) & 1, bz = (corner >> 2) & 1;
+        if ((match[0] >> bx & 1u) && (match[1] >> by & 1u) && (match[2] >> bz & 1u)) {
+            double first = a, second = b;
+            first *= bx ? f1[0] : 1.0 - f1[0];
+            first *= by ? f1[1] : 1.0 - f1[1];
+            first *= bz ? f1[2] : 1.0 - f1[2];
+            second *= bx ? f2[0] : 1.0 - f2[0];
+            second *= by ? f2[1] : 1.0 - f2[1];
+            second *= bz ? f2[2] : 1.0 - f2[2];
+            result += first + second;
+        }
+    }
+    return result;
+}
+
+// The same fixed-order gather for cell-Gauss integration (reference get_gather with
+// cell_gauss, projection_adjoint.py:105-146): each candidate ray's cell walk from its entry,
+// two Gauss nodes per segment weighted by cotangent |e - s| radius.  The walk of every ray
+// was validated when the plan was written.
+template <typename TSeed, typename TOut>
+__global__ void __launch_bounds__(kGatherThreads) k_gather_cells(GatherArgs a, const double* __restrict__ plan,
+                                                                 const TSeed* __restrict__ cotangent,
+                                                                 TOut* __restrict__ out, int accumulate)
+{
+    const int64_t voxel = (int64_t)blockIdx.x * kGatherThreads + threadIdx.x;
+    const int shape[3] = {a.grid.nx, a.grid.ny, a.grid.nz};
+    const int64_t voxels = (int64_t)shape[0] * shape[1] * shape[2];
+    if (voxel >= voxels) return;
+    const int index[3] = {(int)(voxel % shape[0]), (int)((voxel / shape[0]) % shape[1]),
+                          (int)(voxel / ((int64_t)shape[0] * shape[1]))};
+    double lower[3], upper[3];
+    voxel_support(index, shape, lower, upper);
+    FieldDims dims;
+    dims.init(a.grid);
+    const int rays_per_view = a.rows * a.cols;
+    const double* records = plan + (int64_t)a.views * kGatherHeaderWords;
+    const int64_t limit = (int64_t)shape[0] + shape[1] + shape[2] + 1;
+    TOut value = accumulate ? out[voxel] : (TOut)0.0;
+    bool running = accumulate != 0;
+    for (int view = 0; view < a.views; ++view) {
+        const Rect rect = pixel_bounds(plan + (int64_t)view * kGatherHeaderWords, lower, upper, a.rows, a.cols);
+        double total = 0.0;
+        for (int row = rect.first_row; row < rect.last_row; ++row) {
+            for (int col = rect.first_col; col < rect.last_col; ++col) {
+                const int64_t ray_index = (int64_t)view * rays_per_view + row * a.cols + col;
+                const double seed = (double)cotangent[ray_index];
+                if (seed == 0.0) continue;
+                const double* rec = records + ray_index * kGatherRayWords;
+                const double lo = rec[kRayLower], hi = rec[kRayUpper];
+                if (hi - lo <= 0.0) continue;
+                Ray64 r;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    r.origin[k] = rec[kRayOrigin + k];
+                    r.direction[k] = rec[kRayDirection + k];
+                }
+                const double factor = seed * rec[kRayLength];
+                CellWalk64 walk;
+                walk.begin(r, lo, hi, shape);
+                double start = lo;
+                for (int64_t n = 0; start < hi && n < limit; ++n) {
+                    GaussSegment s;
+                    walk.segment(r, start, dims, s);
+                    if (s.end <= start) break;
+                    double vf = factor * s.radius;
+                    if (!isfinite(factor)) vf = range_product(seed, rec[kRayLength], s.radius);
+                    if (s.shared) {
+                        total += cell_terms(s, shape, index, vf);
+                    } else {
+                        total += point_terms(s.first, shape, index, vf);
+                        total += point_terms(s.second, shape, index, vf);
+                    }
+                    start = s.end;
+                    walk.advance(r, shape, s.end, hi);
+                }
+            }
+        }
+        value = running ? (TOut)(total + (double)value) : (TOut)total;
+        running = true;
+    }
+    out[voxel] = value;
+    if (!isfinite((double)value)) atomicOr(a.status + a.view_begin, 2);
+}
+
 // Per-voxel work of a plan (reference get_count_gather_work): candidate rays, sample nodes,
 // voxels whose candidate rectangle exceeds `max_rays` in some view, and fallback voxels.
 __global__ void __launch_bounds__(kGatherThreads) k_gather_count(GatherArgs a, const double* __restrict__ plan,
@@ -502,18 +644,24 @@ cudaError_t launch_gather(const GatherArgs& a, const double* plan, const void* c
 {
     const int64_t voxels = (int64_t)a.grid.nx * a.grid.ny * a.grid.nz;
     const unsigned blocks = (unsigned)((voxels + kGatherThreads - 1) / kGatherThreads);
+    auto run = [&](auto seed_type, auto out_type) {
+        using TS = decltype(seed_type);
+        using TO = decltype(out_type);
+        if (a.cells)
+            k_gather_cells<TS, TO><<<blocks, kGatherThreads, 0, stream>>>(
+                a, plan, static_cast<const TS*>(cotangent), static_cast<TO*>(out), accumulate);
+        else
+            k_gather<TS, TO><<<blocks, kGatherThreads, 0, stream>>>(
+                a, plan, static_cast<const TS*>(cotangent), static_cast<TO*>(out), accumulate);
+    };
     if (seed_dtype == DPT_F64 && out_dtype == DPT_F64)
-        k_gather<double, double><<<blocks, kGatherThreads, 0, stream>>>(
-            a, plan, static_cast<const double*>(cotangent), static_cast<double*>(out), accumulate);
+        run(double{}, double{});
     else if (seed_dtype == DPT_F64)
-        k_gather<double, float><<<blocks, kGatherThreads, 0, stream>>>(
-            a, plan, static_cast<const double*>(cotangent), static_cast<float*>(out), accumulate);
+        run(double{}, float{});
     else if (out_dtype == DPT_F64)
-        k_gather<float, double><<<blocks, kGatherThreads, 0, stream>>>(
-            a, plan, static_cast<const float*>(cotangent), static_cast<double*>(out), accumulate);
+        run(float{}, double{});
     else
-        k_gather<float, float><<<blocks, kGatherThreads, 0, stream>>>(
-            a, plan, static_cast<const float*>(cotangent), static_cast<float*>(out), accumulate);
+        run(float{}, float{});
     return cudaGetLastError();
 }
 

@@ -48,13 +48,14 @@ constexpr int kGatherColumnError = 0, kGatherRowError = 1, kGatherPointError = 2
               kGatherCoefficients = 6, kGatherCone = 18;
 constexpr int kGatherRayWords = 16;
 constexpr int kRayOrigin = 0, kRayDirection = 3, kRayLength = 6, kRayLower = 7, kRaySpan = 8, kRayStep = 9,
-              kRayError = 10;
+              kRayError = 10, kRayUpper = 13;
 
 struct GatherArgs {
     Grid grid;
     int views;       // views of the plan (and of this call)
     int view_begin;  // first absolute view
     int rows, cols, samples, ray_kind;
+    int cells;       // cell-Gauss integration (DPT_ARITH_CELLS) instead of midpoint samples
     const double* poses;       // absolute view indexing
     const double* view_table;  // absolute view indexing
     const double* ray_sources;

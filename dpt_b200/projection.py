@@ -647,7 +647,8 @@ def _gather_metadata(workspace: ProjectionWorkspace) -> tuple:
 
 
 def _gather_problem(workspace: ProjectionWorkspace) -> N.Problem:
-    return workspace.plan.problem(workspace.spec.samples_per_ray, N.ARITH_F64, image_dtype=workspace.spec.image_code)
+    arith = N.ARITH_CELLS if workspace.spec.integration == "cell_gauss" else N.ARITH_F64
+    return workspace.plan.problem(workspace.spec.samples_per_ray, arith, image_dtype=workspace.spec.image_code)
 
 
 @dataclass(frozen=True, eq=False)
@@ -738,7 +739,8 @@ def projection_adjoint_gather(pose, *, cotangent: torch.Tensor, workspace: Proje
                               accumulate: bool = False, validate: Literal["once", "always", "never"] | None = None,
                               max_work: int = 10_000_000) -> torch.Tensor:
     """``out_mu[v] = sum_p A(pose)[p, v] cotangent[p]``: the fixed-pose transpose of the strict
-    FP64 midpoint projection, gathered per voxel in a fixed order (views ascending, each
+    FP64 projection (midpoint, or cell-Gauss with a raw pose), gathered per voxel in a fixed
+    order (views ascending, each
     view's FP64 sum added to the running value; then rows, columns, samples ascending), so it
     is bitwise reproducible (reference python/dpt/projection.py:1250-1405).
 
@@ -758,10 +760,9 @@ def projection_adjoint_gather(pose, *, cotangent: torch.Tensor, workspace: Proje
     plan = pose if isinstance(pose, PreparedProjectionAdjoint) else None
     if plan is not None and (plan.workspace is not workspace or plan.metadata != _gather_metadata(workspace)):
         raise ContractError("prepared adjoint belongs to its original workspace configuration")
-    if plan is None and spec.integration != "midpoint":
-        raise ContractError("the deterministic gather integrates with midpoint samples")
     voxels, pixels = workspace.plan.grid.voxels, workspace.plan.rays
-    work = plan.work_bound if plan is not None else voxels * pixels * spec.samples_per_ray
+    nodes = 2 * (sum(workspace.plan.grid.shape) + 1) if spec.integration == "cell_gauss" else spec.samples_per_ray
+    work = plan.work_bound if plan is not None else voxels * pixels * nodes
     if work > max_work:
         raise ContractError(f"deterministic gather needs at most {work} voxel/ray quadrature evaluations; "
                             f"max_work is {max_work}")

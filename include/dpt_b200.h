@@ -268,7 +268,8 @@ int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_rays* rays, co
 
 /* ---------------------------------------------------------------------------------------
  * Deterministic adjoint gather: out[v] = sum_p A[p, v] cotangent[p] for the strict FP64
- * midpoint projection (arith DPT_ARITH_F64), one thread per voxel summing in FP64 in a fixed
+ * projection, midpoint (arith DPT_ARITH_F64) or cell-Gauss (DPT_ARITH_CELLS; the plan of such
+ * a problem validates every ray's cell walk and is not counted), one thread per voxel summing in FP64 in a fixed
  * order (views ascending, each view's sum added to the running value; then detector rows,
  * columns and samples ascending), so the result is bitwise reproducible.  A plan holds the
  * rays of views [view_begin, view_begin + view_count) of `rays` and their culling metrics;

@@ -64,6 +64,8 @@ def library():
         lib.oracle_check_pose.restype = ctypes.c_int
         lib.oracle_gather.argtypes = [P, V, V, V, V, V, V, ctypes.c_int, ctypes.c_int, V, ctypes.c_int]
         lib.oracle_gather.restype = ctypes.c_int
+        lib.oracle_gather_cells.argtypes = lib.oracle_gather.argtypes
+        lib.oracle_gather_cells.restype = ctypes.c_int
         _lib = lib
     return _lib
 
@@ -161,16 +163,18 @@ def vjp(plan, field, poses, cotangent, *, samples: int, flags: int, arith: int =
 
 
 def gather(plan, poses, cotangent, *, samples: int, image_dtype: int = F64, out_dtype: int = F64,
-           out=None, accumulate: bool = False, threads: int = 0):
-    """Deterministic all-ray adjoint gather of the strict FP64 midpoint operator: per voxel,
-    views ascending, all rays and samples in order.  Returns (volume, status bit word)."""
-    call = _call(plan, samples, ARITH_F64, F32, image_dtype, poses)
+           out=None, accumulate: bool = False, cells: bool = False, threads: int = 0):
+    """Deterministic all-ray adjoint gather of the strict FP64 midpoint operator (or, with
+    ``cells``, of cell-Gauss integration): per voxel, views ascending, all rays and samples (or
+    cell segments) in order.  Returns (volume, status bit word)."""
+    call = _call(plan, samples, ARITH_CELLS if cells else ARITH_F64, F32, image_dtype, poses)
     seed = np.ascontiguousarray(cotangent, dtype=np.float64 if image_dtype == F64 else np.float32).reshape(-1)
     voxels = int(np.prod(plan.grid.shape))
     dtype = np.float64 if out_dtype == F64 else np.float32
     volume = np.zeros(voxels, dtype=dtype) if out is None else np.ascontiguousarray(out, dtype=dtype).reshape(-1).copy()
     status = np.zeros(1, dtype=np.int32)
-    code = library().oracle_gather(
+    function = library().oracle_gather_cells if cells else library().oracle_gather
+    code = function(
         ctypes.byref(call.problem), _ptr(call.poses), _ptr(call.table), _ptr(call.sources),
         _ptr(call.endpoints), _ptr(seed), _ptr(volume), out_dtype, int(accumulate), _ptr(status), threads,
     )

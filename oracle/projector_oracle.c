@@ -2024,3 +2024,105 @@ int oracle_gather(const dpt_problem* p, const double* poses, const double* view_
     status[0] |= bits;
     return 0;
 }
+
+/* product3 (numerics.py:11-52) */
+static double range_product3(double a, double b, double c)
+{
+    if (!isfinite(a) || !isfinite(b) || !isfinite(c)) return a * b * c;
+    if (a == 0.0 || b == 0.0 || c == 0.0) return 0.0;
+    int ea, eb, ec;
+    double ma = frexp(a, &ea), mb = frexp(b, &eb), mc = frexp(c, &ec);
+    return ldexp(ma * mb * mc, ea + eb + ec);
+}
+
+/* cell_contribution (projection_adjoint.py:48-70): both Gauss nodes of a shared cell, per
+ * matching corner first + second */
+static double cell_contribution(int64_t voxel, const segment_t* s, const int* shape, double seed)
+{
+    double result = 0.0, f1[3], f2[3];
+    fraction64(s->first_point, s->lower, shape, f1);
+    fraction64(s->second_point, s->lower, shape, f2);
+    for (int c = 0; c < 8; ++c) {
+        if (corner_index(s->lower, shape, c) != voxel) continue;
+        const double first = scaled_corner64(f1, c, inside64(s->first_point, shape) ? seed : 0.0);
+        const double second = scaled_corner64(f2, c, inside64(s->second_point, shape) ? seed : 0.0);
+        result += first + second;
+    }
+    return result;
+}
+
+/* get_gather with cell_gauss (projection_adjoint.py:105-146): every ray's cell segments, views
+ * summed as oracle_gather does. */
+int oracle_gather_cells(const dpt_problem* p, const double* poses, const double* view_table,
+                        const double* sources, const double* endpoints, const void* cotangent, void* out,
+                        int out_dtype, int accumulate, int32_t* status, int threads)
+{
+    const int shape[3] = {p->nx, p->ny, p->nz};
+    const int64_t voxels = (int64_t)p->nx * p->ny * p->nz, per_view = (int64_t)p->rows * p->cols;
+    int bits = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bits)
+#endif
+    for (int64_t voxel = 0; voxel < voxels; ++voxel) {
+        double value = 0.0;
+        int running = accumulate;
+        if (accumulate) value = out_dtype == DPT_F64 ? ((double*)out)[voxel] : (double)((float*)out)[voxel];
+        for (int view = 0; view < p->views; ++view) {
+            double total = 0.0;
+            for (int64_t pixel = 0; pixel < per_view; ++pixel) {
+                double source[3], end[3];
+                ray_t ray;
+                ray_endpoints(p, view_table, sources, endpoints, view, pixel, source, end);
+                ray_setup(p, poses + 12 * view, source, end, &ray.r);
+                if (!valid_ray(&ray.r)) {
+                    bits |= 2;
+                    continue;
+                }
+                const double seed = (double)load_image(p, cotangent, (int64_t)view * per_view + pixel);
+                if (seed == 0.0) continue;
+                clip64(ray.r.origin, ray.r.direction, shape, &ray.iv64);
+                const interval64_t* iv = &ray.iv64;
+                if (iv->upper - iv->lower <= 0.0) continue;
+                const double factor = seed * ray.r.length;
+                cells_t t;
+                begin_cells(&ray.r, iv, shape, &t);
+                double start = iv->lower;
+                int64_t segments = 0, limit = (int64_t)shape[0] + shape[1] + shape[2] + 1;
+                while (start < iv->upper && segments < limit) {
+                    segment_t s;
+                    cell_segment(&ray.r, &t, start, shape, &s);
+                    if (s.end <= start) {
+                        bits |= 2;
+                        break;
+                    }
+                    if (!finite3(s.first_point) || !finite3(s.second_point)) bits |= 2;
+                    double vf = factor * s.radius;
+                    if (!isfinite(factor)) vf = range_product3(seed, ray.r.length, s.radius);
+                    if (s.shared) {
+                        total += cell_contribution(voxel, &s, shape, vf);
+                    } else {
+                        total += point_contribution(voxel, s.first_point, shape, vf);
+                        total += point_contribution(voxel, s.second_point, shape, vf);
+                    }
+                    start = s.end;
+                    advance_cells(&t, &ray.r, shape, s.end, iv->upper);
+                    ++segments;
+                }
+                if (start < iv->upper) bits |= 2;
+            }
+            if (out_dtype == DPT_F64)
+                value = running ? total + value : total;
+            else
+                value = (double)(float)(running ? total + value : total);
+            running = 1;
+        }
+        if (out_dtype == DPT_F64)
+            ((double*)out)[voxel] = value;
+        else
+            ((float*)out)[voxel] = (float)value;
+        if (!isfinite(value)) bits |= 2;
+    }
+    status[0] |= bits;
+    return 0;
+}

@@ -6,8 +6,8 @@ project at ``/root/reference`` (its host code imports without Warp):
 
 Sources used (paths inside the reference project):
   * tests/python/warp_cpu/test_projection_adjoint_gather.py:26-74 ``_metadata`` (scenes
-    "nonsquare", "bundle", "clamped"); the 31-sample midpoint matrix is formed as its
-    ``_matrix`` (:75-96) forms it, from python/dpt/validation/projection.py
+    "nonsquare", "bundle", "clamped"); the 31-sample midpoint and the cell-Gauss matrices are
+    formed as its ``_matrix`` (:75-96) forms them, from python/dpt/validation/projection.py
     ``integrate_sampled_field`` / ``integrate_ray_bundle``
   * tests/python/warp_cpu/test_projection_culled_adjoint.py:91-138 ``_scene`` (kinds "tilted",
     "inside", "negative_depth", "underflow_plane", "tolerated_rotation", "bundle", and the
@@ -59,8 +59,9 @@ def geometry_record(geometry) -> dict:
             "shape": list(geometry.shape)}
 
 
-def scalar_matrix(grid, geometry, pose, samples: int) -> np.ndarray:
-    """Pixels x voxels FP64 midpoint matrix from the reference's scalar oracle."""
+def scalar_matrix(grid, geometry, pose, samples: int | None) -> np.ndarray:
+    """Pixels x voxels FP64 matrix from the reference's scalar oracle: midpoint with `samples`,
+    or the exact piecewise (cell-Gauss) integral for None."""
     matrix = np.empty((geometry.pixels, grid.voxels))
     for voxel in range(grid.voxels):
         basis = [float(index == voxel) for index in range(grid.voxels)]
@@ -91,6 +92,7 @@ def main() -> None:
         cases[name] = {"grid": grid_record(grid), "geometry": geometry_record(geometry),
                        "pose": list(pose.packed()), "samples": 31}
         arrays[f"{name}_matrix"] = scalar_matrix(grid, geometry, pose, 31)
+        arrays[f"{name}_cells_matrix"] = scalar_matrix(grid, geometry, pose, None)
     kinds = ["tilted", "inside", "negative_depth", "underflow_plane", "tolerated_rotation", "bundle"]
     for kind in kinds:
         grid, geometry, pose = culled_tests["_scene"](kind)

@@ -191,3 +191,27 @@ def test_invalid_rays_and_overflowing_zero_weight_corners():
         with pytest.raises(NumericalError):
             projection_adjoint_gather(operator, cotangent=seed, workspace=ws, out_mu=out)
         assert np.isnan(out.cpu().numpy()).all()
+
+
+@pytest.mark.parametrize("name", ["gather_nonsquare", "gather_bundle", "gather_clamped"])
+@pytest.mark.parametrize("precision", ["float32", "float64"])
+def test_cell_gauss_gather_matches_oracle_and_reference_exact_matrix(name, precision):
+    grid, geometry, pose_np, _ = gather_scene(name)
+    spec = ProjectionSpec(31, active_pose=False, active_volume=True, precision="float64",
+                          integration="cell_gauss", field_domain="signed_linear")
+    ws = prepare_projection(grid, geometry, spec, device=DEVICE)
+    pose = torch.tensor(pose_np, device=DEVICE)
+    matrix = np.load(__import__("scenes").GOLDEN / "gather.npz")[f"{name}_cells_matrix"]
+    rng = np.random.default_rng(17)
+    code = O.F64 if precision == "float64" else O.F32
+    for _ in range(3):
+        seeds = rng.uniform(-1, 1, ws.plan.rays)
+        cot = torch.tensor(seeds, device=DEVICE).reshape(ws.plan.image_shape)
+        out = projection_adjoint_gather(pose, cotangent=cot, workspace=ws, volume_gradient_precision=precision)
+        expected, status = O.gather(ws.plan, pose_np, seeds, samples=31, cells=True, out_dtype=code)
+        assert status == 0
+        assert out.cpu().numpy().reshape(-1).tobytes() == expected.tobytes()
+        if precision == "float64":
+            np.testing.assert_allclose(out.cpu().numpy().reshape(-1), matrix.T @ seeds, rtol=2e-12, atol=2e-12)
+    with pytest.raises(ContractError, match="strict float64 midpoint"):
+        prepare_projection_adjoint(pose, workspace=ws)

@@ -73,3 +73,20 @@ def test_overflowing_zero_weight_corner_keeps_the_canonical_failure():
     gradient, status = O.gather(plan, pose, np.array([1e308]), samples=1)
     assert status & 2
     assert np.isnan(gradient).all()
+
+
+@pytest.mark.parametrize("name", ["gather_nonsquare", "gather_bundle", "gather_clamped"])
+def test_cell_gauss_gather_matches_reference_exact_matrix(name):
+    grid, geometry, pose, _ = gather_scene(name)
+    plan = plan_rays(grid, geometry)
+    matrix = np.load(__import__("scenes").GOLDEN / "gather.npz")[f"{name}_cells_matrix"]
+    rng = np.random.default_rng(91)
+    for _ in range(5):
+        values = rng.uniform(-1, 1, grid.voxels).astype(np.float32)
+        seeds = rng.uniform(-1, 1, plan.rays)
+        gradient, status = O.gather(plan, pose, seeds, samples=1, cells=True)
+        assert status == 0
+        np.testing.assert_allclose(gradient, matrix.T @ seeds, rtol=2e-12, atol=2e-12)
+        image, _ = O.forward(plan, values, pose, samples=1, arith=O.ARITH_CELLS, image_dtype=O.F64)
+        left, right = math.fsum(image * seeds), math.fsum(values.astype(np.float64) * gradient)
+        assert abs(left - right) < 2e-12 * max(1.0, abs(left), abs(right))
