@@ -58,7 +58,8 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--storage", choices=("float32", "bfloat16", "float16"), default="float32")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--seed", type=int, default=20261203)
-    parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise"), default="iteration",
+    parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise", "gather"),
+                        default="iteration",
                         help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
     parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
     parser.add_argument("--slots", type=int, default=4, help="serving mode: concurrent request streams")
@@ -765,6 +766,68 @@ def run_pointwise(args) -> None:
                       "results": results, "cpu_baseline": cpu}), flush=True)
 
 
+def run_gather(args) -> None:
+    """Deterministic adjoint gather of the strict FP64 midpoint projector on a scan of
+    ``--views`` cone views of ``--detector``^2 pixels over a ``--size``^3 chest phantom grid
+    (S = ``--samples``): plan preparation once, then the culled per-voxel gather timed with
+    CUDA events over ``--steps`` launches, beside the strict FP64 scatter VJP of the same
+    cotangent.  Reports voxel-views, visited (voxel, sample) nodes and per-voxel node rate."""
+    import numpy as np
+    import torch
+
+    from dpt_b200.geometry import ConeBeamIntrinsics
+    from dpt_b200.phantoms import centred_grid
+    from dpt_b200.projection import (ProjectionSpec, prepare_projection, prepare_projection_adjoint,
+                                     projection_adjoint_gather, projection_vjp)
+
+    device = torch.device("cuda:0")
+    spacing = 0.8 * 256.0 / args.size
+    grid = centred_grid((args.size,) * 3, (spacing,) * 3)
+    geometry = ConeBeamIntrinsics(1000.0, 1500.0, (args.detector, args.detector),
+                                  (0.8 * 512.0 / args.detector,) * 2).batch(
+        tuple(2.0 * math.pi * k / args.views for k in range(args.views)))
+    spec = ProjectionSpec(args.samples, active_pose=False, active_volume=True, precision="float64",
+                          field_domain="signed_linear", validate="never")
+    ws = prepare_projection(grid, geometry, spec, device=device)
+    poses = torch.tensor(np.tile([1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0, 0, 0, 0], (args.views, 1)), device=device)
+    plan = prepare_projection_adjoint(poses, workspace=ws, max_work=2**62, max_prepare_voxels=2**31,
+                                      max_rays_per_voxel=1 << 20, max_bytes=1 << 40)
+    generator = torch.Generator(device=device).manual_seed(args.seed)
+    cot = torch.randn(ws.plan.image_shape, dtype=torch.float64, device=device, generator=generator)
+    out = torch.empty(grid.shape, dtype=torch.float64, device=device)
+    field = torch.zeros(grid.shape, dtype=torch.float32, device=device)
+
+    def timed(fn, steps):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(steps):
+            fn()
+        end.record()
+        end.synchronize()
+        return start.elapsed_time(end) / 1e3 / steps
+
+    gather_s = timed(lambda: projection_adjoint_gather(plan, cotangent=cot, workspace=ws, out_mu=out,
+                                                       max_work=2**62, validate="never"), args.steps)
+    first = out.clone()
+    projection_adjoint_gather(plan, cotangent=cot, workspace=ws, out_mu=out, max_work=2**62, validate="never")
+    repeatable = bool(torch.equal(first, out))
+    scatter_s = timed(lambda: projection_vjp(field, poses, cotangent=cot, workspace=ws, pose_gradient=None,
+                                             volume_gradient_precision="float64"), args.steps)
+    voxel_views = grid.voxels * args.views
+    print(json.dumps({
+        "metric": "deterministic adjoint gather, strict FP64 midpoint", "unit": "voxel-views/s",
+        "value": round(voxel_views / gather_s, 1),
+        "config": {"workload": f"{args.size}^3 grid, {args.views} cone views {args.detector}^2, S={args.samples}",
+                   "plan": {"candidate_rays": plan.candidate_rays, "quadrature_nodes": plan.quadrature_nodes,
+                            "fallback_voxels": plan.fallback_voxels, "device_bytes": plan.device_bytes}},
+        "gather_ms": round(gather_s * 1e3, 3), "nodes_per_s": round(plan.quadrature_nodes / gather_s, 1),
+        "repeatable_bitwise": repeatable,
+        "scatter_vjp_fp64_ms": round(scatter_s * 1e3, 3)}), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -775,6 +838,8 @@ def main() -> None:
         run_precision(args)
     elif args.mode == "pointwise":
         run_pointwise(args)
+    elif args.mode == "gather":
+        run_gather(args)
     else:
         run_gpu(args)
 

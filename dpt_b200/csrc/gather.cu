@@ -25,9 +25,25 @@ namespace dpt {
 namespace {
 
 constexpr int kGatherThreads = 128;
+#ifndef DPT_GATHER_MIN_BLOCKS
+#define DPT_GATHER_MIN_BLOCKS 6  // resident 128-thread blocks per SM the midpoint gather is compiled for
+#endif
 
-__device__ __forceinline__ double down(double x) { return nextafter(x, -INFINITY); }
-__device__ __forceinline__ double up(double x) { return nextafter(x, INFINITY); }
+// The adjacent double below / above x (nextafter toward -inf / +inf): one integer step of the
+// bit pattern, with NaN and the infinity in the direction of travel unchanged and a zero
+// stepping to the smallest subnormal.
+__device__ __forceinline__ double down(double x)
+{
+    if (x != x || x == -INFINITY) return x;
+    if (x == 0.0) return -4.9406564584124654e-324;
+    return __longlong_as_double(__double_as_longlong(x) + (x > 0.0 ? -1 : 1));
+}
+__device__ __forceinline__ double up(double x)
+{
+    if (x != x || x == INFINITY) return x;
+    if (x == 0.0) return 4.9406564584124654e-324;
+    return __longlong_as_double(__double_as_longlong(x) + (x > 0.0 ? 1 : -1));
+}
 
 // Enclosure of the real dot product a . b of stored FP64 vectors (every primitive rounded
 // outward; reference enclosed_dot).
@@ -398,7 +414,7 @@ __device__ __forceinline__ double point_terms(const double* q, const int* shape,
 }
 
 template <typename TSeed, typename TOut>
-__global__ void __launch_bounds__(kGatherThreads) k_gather(GatherArgs a, const double* __restrict__ plan,
+__global__ void __launch_bounds__(kGatherThreads, DPT_GATHER_MIN_BLOCKS) k_gather(GatherArgs a, const double* __restrict__ plan,
                                                            const TSeed* __restrict__ cotangent,
                                                            TOut* __restrict__ out, int accumulate)
 {
@@ -435,8 +451,9 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(GatherArgs a, const d
                 const double o[3] = {ray[kRayOrigin], ray[kRayOrigin + 1], ray[kRayOrigin + 2]};
                 const double d[3] = {ray[kRayDirection], ray[kRayDirection + 1], ray[kRayDirection + 2]};
                 const double base = ray[kRayLower], step = ray[kRayStep];
-                for (int s = first; s < last; ++s) {
-                    const double position = fma((double)s + 0.5, step, base);
+                double offset = (double)first + 0.5;  // s + 1/2, exact
+                for (int s = first; s < last; ++s, offset += 1.0) {
+                    const double position = fma(offset, step, base);
                     const double q[3] = {fma(position, d[0], o[0]), fma(position, d[1], o[1]),
                                          fma(position, d[2], o[2])};
                     total += point_terms(q, shape, index, scale);
