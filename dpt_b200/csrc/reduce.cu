@@ -59,19 +59,23 @@ __device__ __forceinline__ int axis_sources(int x, int n, int* cells, int* bits)
     return count;
 }
 
-// Fold tile: 16 x 4 x 4 voxels per 256-thread block.  The cells that touch those voxels are
-// [x0-1, x0+16) x [y0-1, y0+4) x [z0-1, z0+4): 17 x 5 x 5 records of 32 bytes, loaded into
-// shared memory with coalesced 16-byte loads (about 1.7 record reads per voxel).
-constexpr int kFoldX = 16, kFoldY = 4, kFoldZ = 4;
+// Fold tile: 16 x 4 x 16 voxels per 256-thread block, each thread folding four voxels spaced
+// 4 apart in z.  The cells that touch those voxels are [x0-1, x0+16) x [y0-1, y0+4) x
+// [z0-1, z0+16): 17 x 5 x 17 records of 32 bytes (1.4 record reads per voxel), loaded with
+// coalesced 16-byte loads and stored corner-major in shared memory (one FP32 array per
+// corner), so that the 32 lanes of a warp, which fold consecutive voxels in x, read 32
+// consecutive words of one corner array: no bank conflicts.
+constexpr int kFoldX = 16, kFoldY = 4, kFoldZ = 16, kFoldPasses = 4;
 constexpr int kHaloX = kFoldX + 1, kHaloY = kFoldY + 1, kHaloZ = kFoldZ + 1;
 constexpr int kHaloCells = kHaloX * kHaloY * kHaloZ;
+constexpr size_t kFoldShared = 8 * kHaloCells * sizeof(float);  // 46,240 bytes
 
 template <typename G>
 __global__ void __launch_bounds__(256) k_fold(int nx, int ny, int nz, const float* __restrict__ acc,
                                               double* __restrict__ total, int accumulate_total,
                                               G* __restrict__ gradient, int32_t* status)
 {
-    __shared__ float4 cells[kHaloCells][2];
+    extern __shared__ float corners[];  // [8][kHaloCells]
     const int tiles_x = (nx + kFoldX - 1) / kFoldX, tiles_y = (ny + kFoldY - 1) / kFoldY;
     const int tile = blockIdx.x;
     const int tz = tile / (tiles_x * tiles_y), rest = tile - tz * tiles_x * tiles_y;
@@ -86,37 +90,45 @@ __global__ void __launch_bounds__(256) k_fold(int nx, int ny, int nz, const floa
         float4 value = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (gx >= 0 && gy >= 0 && gz >= 0 && gx < nx && gy < ny && gz < nz)
             value = __ldg(records + 2 * (((int64_t)gz * ny + gy) * nx + gx) + half);
-        cells[c][half] = value;
+        float* base = corners + 4 * half * kHaloCells + c;
+        base[0] = value.x;
+        base[kHaloCells] = value.y;
+        base[2 * kHaloCells] = value.z;
+        base[3 * kHaloCells] = value.w;
     }
     __syncthreads();
-    const int lx = threadIdx.x % kFoldX, ly = (threadIdx.x / kFoldX) % kFoldY, lz = threadIdx.x / (kFoldX * kFoldY);
-    const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+    const int lx = threadIdx.x % kFoldX, ly = (threadIdx.x / kFoldX) % kFoldY, lz0 = threadIdx.x / (kFoldX * kFoldY);
+    const int x = x0 + lx, y = y0 + ly;
     bool bad = false;
-    if (x < nx && y < ny && z < nz) {
-        int cxs[2], bxs[2], cys[2], bys[2], czs[2], bzs[2];
+    if (x < nx && y < ny) {
+        int cxs[2], bxs[2], cys[2], bys[2];
         const int kx = axis_sources(x, nx, cxs, bxs);
         const int ky = axis_sources(y, ny, cys, bys);
-        const int kz = axis_sources(z, nz, czs, bzs);
-        double sum = 0.0;
-        for (int iz = 0; iz < kz; ++iz)
-            for (int iy = 0; iy < ky; ++iy)
-                for (int ix = 0; ix < kx; ++ix) {
-                    const int c = ((czs[iz] - z0 + 1) * kHaloY + (cys[iy] - y0 + 1)) * kHaloX + (cxs[ix] - x0 + 1);
-                    const int corner = bxs[ix] | (bys[iy] << 1) | (bzs[iz] << 2);
-                    const float4 q = cells[c][corner >> 2];
-                    const int k = corner & 3;
-                    sum += (double)(k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w);
-                }
-        const int64_t index = ((int64_t)z * ny + y) * nx + x;
-        double value = sum;
-        if (total) {
-            if (accumulate_total) value += total[index];
-            total[index] = value;
-        }
-        if (gradient) {
-            const G out = (G)value;
-            gradient[index] = out;
-            bad = !isfinite(out);
+#pragma unroll
+        for (int pass = 0; pass < kFoldPasses; ++pass) {
+            const int z = z0 + lz0 + pass * (kFoldZ / kFoldPasses);
+            if (z >= nz) break;
+            int czs[2], bzs[2];
+            const int kz = axis_sources(z, nz, czs, bzs);
+            double sum = 0.0;
+            for (int iz = 0; iz < kz; ++iz)
+                for (int iy = 0; iy < ky; ++iy)
+                    for (int ix = 0; ix < kx; ++ix) {
+                        const int c = ((czs[iz] - z0 + 1) * kHaloY + (cys[iy] - y0 + 1)) * kHaloX + (cxs[ix] - x0 + 1);
+                        const int corner = bxs[ix] | (bys[iy] << 1) | (bzs[iz] << 2);
+                        sum += (double)corners[corner * kHaloCells + c];
+                    }
+            const int64_t index = ((int64_t)z * ny + y) * nx + x;
+            double value = sum;
+            if (total) {
+                if (accumulate_total) value += total[index];
+                total[index] = value;
+            }
+            if (gradient) {
+                const G out = (G)value;
+                gradient[index] = out;
+                bad = bad || !isfinite(out);
+            }
         }
     }
     const unsigned any = __ballot_sync(0xffffffffu, bad);
@@ -141,10 +153,10 @@ cudaError_t launch_fold(const dpt_problem& p, float* accumulator, double* total,
     const unsigned blocks = (unsigned)(((p.nx + kFoldX - 1) / kFoldX) * ((p.ny + kFoldY - 1) / kFoldY) *
                                        ((p.nz + kFoldZ - 1) / kFoldZ));
     if (gradient_dtype == DPT_F64)
-        k_fold<double><<<blocks, 256, 0, stream>>>(p.nx, p.ny, p.nz, accumulator, total,
+        k_fold<double><<<blocks, 256, kFoldShared, stream>>>(p.nx, p.ny, p.nz, accumulator, total,
                                                    accumulate_total, static_cast<double*>(gradient), status);
     else
-        k_fold<float><<<blocks, 256, 0, stream>>>(p.nx, p.ny, p.nz, accumulator, total,
+        k_fold<float><<<blocks, 256, kFoldShared, stream>>>(p.nx, p.ny, p.nz, accumulator, total,
                                                   accumulate_total, static_cast<float*>(gradient), status);
     cudaError_t error = cudaGetLastError();
     if (error == cudaSuccess && clear)
