@@ -12,8 +12,8 @@
 //   F32C - FP64 setup and clip; FP32 marching p_i = entry + (i+0.5) step_vector (the mixed
 //          recurrence of python/dpt/kernels/projection.py:368-392); the samples of each cell
 //          run summed in closed form from the cell's trilinear polynomial, the run sums added
-//          with Kahan compensation and scaled by length*step in FP64 (the precision form of
-//          this build, no reference counterpart).
+//          with Kahan compensation and scaled by length*step in FP64 (this library's
+//          precision form, no reference counterpart).
 //
 // Samples inside the support form one run; within it the interior run (0 <= p < n-1 on every
 // axis) skips the clamps of the cell coordinate.  Both are exact rewrites of the per-sample

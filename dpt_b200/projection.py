@@ -49,7 +49,7 @@ _ARITH = {"float32": N.ARITH_F32, "float64": N.ARITH_F64, "mixed_float32": N.ARI
 @dataclass(frozen=True, slots=True)
 class ProjectionSpec:
     """Quadrature and arithmetic of one projector (reference ``ProjectionSpec``,
-    python/dpt/projection.py:67-140, with this build's launch options).
+    python/dpt/projection.py:67-140, with this package's launch options).
 
     ``integration``: ``"midpoint"`` uses ``samples_per_ray`` clipped midpoints;
     ``"cell_gauss"`` splits the ray at every interpolation plane and integrates each
@@ -58,7 +58,7 @@ class ProjectionSpec:
     ``"float32"`` the reference FP32 projector (FP64 ray setup, FP32 clip, interpolation
     and serial ray sum; FP32 storage); ``"mixed_float32"`` FP32 marching and corner
     weights with FP64 products and sums, ``"fast_float32"`` the same with an FP32 cell
-    sum (both fixed-pose); ``"compensated"`` this build's precision form for FP16/BF16
+    sum (both fixed-pose); ``"compensated"`` this package's precision form for FP16/BF16
     storage (closed-form sums over the cell runs, compensated FP32 ray sum).
     ``storage_precision`` FP32, FP16 or BF16 field storage (decoded exactly on the
     device); ``field_domain`` ``"physical"`` (finite, non-negative attenuation) or

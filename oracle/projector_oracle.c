@@ -31,7 +31,7 @@
  *
  * The DPT_ARITH_F32C form (FP64 clip, FP32 marching, trilinear-polynomial samples,
  * blocked compensated sum, moment-based scatter) has no reference counterpart: it is
- * the storage-precision form of this build, restated here from its own definition
+ * the projector library's storage-precision form, restated here from its own definition
  * and checked in the tests against F64.
  */
 #include <math.h>
