@@ -1,6 +1,6 @@
 """Device-resident projection serving with continuous batching.
 
-The reference has no serving layer; this module is the request loop the B200 build
+The reference has no serving layer; this module is the request loop the package
 adds on top of the projector:
 
 * volumes are registered once and stay resident (with their corner-replicated copy);
