@@ -58,7 +58,7 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--storage", choices=("float32", "bfloat16", "float16"), default="float32")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--seed", type=int, default=20261203)
-    parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise", "gather"),
+    parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise", "gather", "panels"),
                         default="iteration",
                         help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
     parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
@@ -828,6 +828,100 @@ def run_gather(args) -> None:
         "scatter_vjp_fp64_ms": round(scatter_s * 1e3, 3)}), flush=True)
 
 
+def run_panels(args) -> None:
+    """Panel kinds and the per-ray pose Jacobian on the full-scan volume: the FP32 forward
+    over ``--views`` views of ``--detector``^2 as cone panels, as parallel panels (each
+    view's rays along its central ray, SDD long) and as cylindrical panels (around each
+    view's source), each in one launch; and, on the cone panels, the per-ray 6-row pose
+    Jacobian (48 FP64 bytes written per ray) beside the per-view pose VJP of the same
+    cotangent.  Rates are realised ray-samples per second (CUDA events, 3 launches after a
+    warm-up)."""
+    import numpy as np
+    import torch
+
+    from dpt_b200.geometry import (BatchedGeometry, ConeBeamIntrinsics, CurvedDetectorGeometry,
+                                   ParallelGeometry)
+    from dpt_b200.phantoms import centred_grid, chest_phantom
+    from dpt_b200.projection import ProjectionSpec, ProjectionWorkspace
+    from dpt_b200.plan import plan_rays
+
+    device = torch.device("cuda:0")
+    spacing = 0.8 * 256.0 / args.size
+    grid = centred_grid((args.size,) * 3, (spacing,) * 3)
+    intrinsics = ConeBeamIntrinsics(1000.0, 1500.0, (args.detector, args.detector),
+                                    (0.8 * 512.0 / args.detector,) * 2)
+    cones = [intrinsics.view(2.0 * math.pi * k / args.views) for k in range(args.views)]
+
+    def parallel(c):
+        centre = [c.origin_mm[k] + 0.5 * (c.shape[1] - 1) * c.spacing_mm[0] * c.u[k]
+                  + 0.5 * (c.shape[0] - 1) * c.spacing_mm[1] * c.v[k] for k in range(3)]
+        axis = [centre[k] - c.source_mm[k] for k in range(3)]
+        norm = math.sqrt(sum(x * x for x in axis))
+        return ParallelGeometry(c.origin_mm, tuple(x / norm for x in axis), 1500.0, c.u, c.v, c.spacing_mm, c.shape)
+
+    def curved(c):
+        # cylinder of radius SDD about the axis through the source along v, centred on the
+        # central ray; pixel (0, 0) sits at arc angle a0 with u tangent there
+        centre = [c.origin_mm[k] + 0.5 * (c.shape[1] - 1) * c.spacing_mm[0] * c.u[k]
+                  + 0.5 * (c.shape[0] - 1) * c.spacing_mm[1] * c.v[k] for k in range(3)]
+        n = [centre[k] - c.source_mm[k] for k in range(3)]
+        norm = math.sqrt(sum(x * x for x in n))
+        n = [x / norm for x in n]
+        radius = 1500.0
+        a0 = -0.5 * (c.shape[1] - 1) * c.spacing_mm[0] / radius
+        row0 = -0.5 * (c.shape[0] - 1) * c.spacing_mm[1]
+        origin = tuple(c.source_mm[k] + radius * (math.cos(a0) * n[k] + math.sin(a0) * c.u[k]) + row0 * c.v[k]
+                       for k in range(3))
+        u = tuple(-math.sin(a0) * n[k] + math.cos(a0) * c.u[k] for k in range(3))
+        return CurvedDetectorGeometry(c.source_mm, origin, u, c.v, c.spacing_mm, c.shape)
+
+    kinds = {
+        "cone": BatchedGeometry(tuple(cones)),
+        "parallel": BatchedGeometry(tuple(parallel(c) for c in cones)),
+        "curved": BatchedGeometry(tuple(curved(c) for c in cones)),
+    }
+    field = torch.tensor(chest_phantom(grid, seed=args.seed), device=device)
+    poses = torch.tensor(np.tile([1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0, 0, 0, 0], (args.views, 1)), device=device)
+
+    def timed(fn, repeats=3):
+        fn()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(repeats):
+            fn()
+        end.record()
+        end.synchronize()
+        return start.elapsed_time(end) / 1e3 / repeats
+
+    results = {}
+    cone_ws = None
+    for name, geometry in kinds.items():
+        ws = ProjectionWorkspace(plan_rays(grid, geometry), ProjectionSpec(args.samples, validate="never"), device)
+        lower, upper, _ = ws.counts(poses)
+        realised = int((upper > lower).sum()) * args.samples
+        seconds = timed(lambda: ws.forward(field, poses))
+        results[name] = {"forward_ms": round(seconds * 1e3, 3), "realised_samples": realised,
+                         "samples_per_s": round(realised / seconds, 1)}
+        if name == "cone":
+            cone_ws = ws
+    cot = torch.randn(cone_ws.plan.image_shape, device=device,
+                      generator=torch.Generator(device=device).manual_seed(args.seed))
+    rays = cone_ws.plan.rays
+    jacobian_s = timed(lambda: cone_ws.pose_sensitivities(field, poses, cot, checked=False))
+    pose_s = timed(lambda: cone_ws.vjp(field, poses, cot, volume=False, pose="tangent"))
+    peak, peak_kind = measured_peak()
+    print(json.dumps({
+        "metric": "panel kinds and per-ray pose Jacobian, FP32 arithmetic", "unit": "ray-samples/s",
+        "config": {"workload": f"{args.size}^3 chest, {args.views} views {args.detector}^2, S={args.samples}"},
+        "forward": results,
+        "per_ray_jacobian": {"ms": round(jacobian_s * 1e3, 3), "rays_per_s": round(rays / jacobian_s, 1),
+                             "output_gbs": round(48 * rays / jacobian_s / 1e9, 1),
+                             "per_view_pose_vjp_ms": round(pose_s * 1e3, 3),
+                             "hbm_peak_gbs": peak, "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs"}}),
+          flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -840,6 +934,8 @@ def main() -> None:
         run_pointwise(args)
     elif args.mode == "gather":
         run_gather(args)
+    elif args.mode == "panels":
+        run_panels(args)
     else:
         run_gpu(args)
 
