@@ -897,7 +897,9 @@ def run_panels(args) -> None:
     results = {}
     cone_ws = None
     for name, geometry in kinds.items():
-        ws = ProjectionWorkspace(plan_rays(grid, geometry), ProjectionSpec(args.samples, validate="never"), device)
+        ws = ProjectionWorkspace(plan_rays(grid, geometry),
+                                 ProjectionSpec(args.samples, precision="float32", sampling_precision="float32",
+                                                validate="never"), device)
         lower, upper, _ = ws.counts(poses)
         realised = int((upper > lower).sum()) * args.samples
         seconds = timed(lambda: ws.forward(field, poses))

@@ -188,7 +188,7 @@ int dpt_b200_forward(const dpt_problem* p, const dpt_rays* r, const void* packed
     if (!aligned(packed, 16)) return DPT_E_ALIGN;
     const int64_t rays_per_view = (int64_t)p->rows * p->cols;
     const size_t element = p->image_dtype == DPT_F64 ? 8 : 4;
-    return chunked(p, r, status, dpt::kBlock, [&](const dpt::RayArgs& a, int32_t first) {
+    return chunked(p, r, status, dpt::kForwardBlock, [&](const dpt::RayArgs& a, int32_t first) {
         char* out = static_cast<char*>(image) + (size_t)first * rays_per_view * element;
         return to_code(dpt::launch_forward(*p, a, packed, out, static_cast<cudaStream_t>(stream)));
     });

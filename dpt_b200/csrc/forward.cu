@@ -20,6 +20,10 @@
 // tests, so every mode keeps its arithmetic bit for bit.
 #include "launch.h"
 
+#ifndef DPT_FORWARD_REUSE
+#define DPT_FORWARD_REUSE 1  // FP32 forward: reload the corners only when the sample enters another cell
+#endif
+
 namespace dpt {
 namespace {
 
@@ -58,7 +62,7 @@ __device__ __forceinline__ bool finite_out(double value)
 }
 
 template <int kArith, class Field, typename Out>
-__global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __restrict__ image)
+__global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, Out* __restrict__ image)
 {
     __shared__ ViewShared vs;
     const int view_local = blockIdx.y;
@@ -118,7 +122,7 @@ __global__ void __launch_bounds__(kBlock) k_forward(RayArgs a, Field f, Out* __r
                         at(i, x, y, z);
                         return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
                     }, ifirst, ilast);
-                    CellCache<Field> cache;
+                    CellCache<Field, DPT_FORWARD_REUSE != 0> cache;
                     auto add = [&](Axis32 X, Axis32 Y, Axis32 Z) {
                         cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
                         float w[8];
@@ -477,9 +481,9 @@ cudaError_t forward_with(const dpt_problem& p, const RayArgs& a, const Field& f,
                          dim3 grid, cudaStream_t stream)
 {
     if (p.image_dtype == DPT_F64)
-        k_forward<kArith, Field, double><<<grid, kBlock, 0, stream>>>(a, f, static_cast<double*>(image));
+        k_forward<kArith, Field, double><<<grid, kForwardBlock, 0, stream>>>(a, f, static_cast<double*>(image));
     else
-        k_forward<kArith, Field, float><<<grid, kBlock, 0, stream>>>(a, f, static_cast<float*>(image));
+        k_forward<kArith, Field, float><<<grid, kForwardBlock, 0, stream>>>(a, f, static_cast<float*>(image));
     return cudaGetLastError();
 }
 
