@@ -1,6 +1,6 @@
 // forward.cu - optical depth and per-ray clip counts.
 //
-// One thread marches one ray; a 256-thread block covers a 16x16 detector tile (each warp
+// One thread marches one ray; a 128-thread block covers a 16x8 detector tile (each warp
 // an 8x4 sub-tile) so the 32 rays of a warp sample neighbouring voxels at every step and
 // their corner loads share L1 lines.  One launch covers every view of a call (blockIdx.y
 // is the view), where the reference launches once per view.
