@@ -40,6 +40,11 @@
 #ifndef DPT_VJP_MIN_BLOCKS_F32C_FORWARD
 #define DPT_VJP_MIN_BLOCKS_F32C_FORWARD 9
 #endif
+// The compensated joint volume + pose pass: 237.9 ms per full scan at eight blocks (64
+// registers, 376 bytes spilled), 247.3 at seven, 252.6 at six, 249.7 at nine, 310.3 at ten.
+#ifndef DPT_VJP_MIN_BLOCKS_F32C_JOINT
+#define DPT_VJP_MIN_BLOCKS_F32C_JOINT 8
+#endif
 #ifndef DPT_VJP_MIN_BLOCKS_F64
 #define DPT_VJP_MIN_BLOCKS_F64 3
 #endif
@@ -125,7 +130,8 @@ struct MomentArgs {
 template <int kArith, class Field, bool kVol, bool kPose, typename Seed, int kMoments = kJointMoments>
 __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                                   ? (kMoments == kStoreMoments ? DPT_VJP_MIN_BLOCKS_F32C_FORWARD
-                                                                               : DPT_VJP_MIN_BLOCKS_F32C)
+                                                     : (kVol && kPose)             ? DPT_VJP_MIN_BLOCKS_F32C_JOINT
+                                                                                   : DPT_VJP_MIN_BLOCKS_F32C)
                                                   : kArith == DPT_ARITH_F32 ? DPT_VJP_MIN_BLOCKS_F32
                                                                             : DPT_VJP_MIN_BLOCKS_F64)
     k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,

@@ -173,9 +173,11 @@ def _forward(field, poses, value, active_volume, active_pose, out=None):
         raise ContractError("out must not share storage with projection inputs")
     entry = workspace(field, value, active_volume, active_pose)
     with torch.no_grad():
-        # a pose that will be differentiated: gather the pose moments in this pass, so the
-        # backward's pose VJP needs no second sampling pass (results are unchanged)
-        return entry.forward(field, poses.contiguous(), out, moments=active_pose and out is None)
+        # a pose that will be differentiated: where the arithmetic prefers it, gather the pose
+        # moments in this pass, so the backward's pose VJP needs no second sampling pass
+        # (results are unchanged either way)
+        return entry.forward(field, poses.contiguous(), out,
+                             moments=active_pose and out is None and entry.moments_preferred())
 
 
 @torch.library.custom_op("dpt::project", mutates_args=(), tags=_TAGS)
