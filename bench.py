@@ -58,7 +58,8 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--storage", choices=("float32", "bfloat16", "float16"), default="float32")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--seed", type=int, default=20261203)
-    parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise", "gather", "panels"),
+    parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise", "gather", "panels",
+                                           "table"),
                         default="iteration",
                         help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
     parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
@@ -924,6 +925,126 @@ def run_panels(args) -> None:
           flush=True)
 
 
+def run_table(args) -> None:
+    """Per-operation device times of the reference's published tables, on B200.
+
+    Full scan (the headline workload: 256^3 chest at 0.8 mm, ``--views`` views of 512^2,
+    S = 1024): forward, volume VJP, per-view pose VJP and the full iteration (forward +
+    joint volume and pose VJP) in the FP32 and strict FP64 forms (the reference's
+    ``fp32`` / ``fp64`` Projector precisions, python/dpt/torch/modules.py:69-228), and the
+    FP64 cell-Gauss form.  Native chest (a synthetic chest on the 512 x 512 x 139 grid at
+    0.7617 x 0.7617 x 2.5 mm standing in for the CT file; three 512^2 views at pi, pi/2 and
+    3 pi/4 with the reference benchmark's geometry rule, SOD = max(1000, 2 diag), SDD =
+    max(1500, 3 diag), detector width 1.05 diag SDD / (SOD - diag/2)): the strict FP64,
+    mixed FP32 and fast FP32 forwards with FP64 output.  Each operation: one warm-up, then
+    ``--steps`` launches, each bracketed by CUDA events with a 256 MiB L2 flush between."""
+    import numpy as np
+    import torch
+
+    from dpt_b200.geometry import ConeBeamIntrinsics
+    from dpt_b200.phantoms import centred_grid, chest_phantom
+    from dpt_b200.plan import plan_rays
+    from dpt_b200.projection import ProjectionSpec, ProjectionWorkspace
+
+    device = torch.device("cuda:0")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        spans = []
+        for _ in range(args.steps):
+            flush.zero_()
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            fn()
+            end.record()
+            spans.append((start, end))
+        torch.cuda.synchronize()
+        times = sorted(s.elapsed_time(e) for s, e in spans)
+        return round(times[len(times) // 2], 3)
+
+    def identity(views):
+        return torch.tensor(np.tile([1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0, 0, 0, 0], (views, 1)), device=device)
+
+    # ---- full scan
+    spacing = 0.8 * 256.0 / args.size
+    grid = centred_grid((args.size,) * 3, (spacing,) * 3)
+    geometry = ConeBeamIntrinsics(1000.0, 1500.0, (args.detector, args.detector),
+                                  (0.8 * 512.0 / args.detector,) * 2).batch(
+        tuple(2.0 * math.pi * k / args.views for k in range(args.views)))
+    plan = plan_rays(grid, geometry)
+    values = torch.tensor(chest_phantom(grid, seed=args.seed), device=device)
+    poses = identity(args.views)
+    cot = torch.randn(plan.image_shape, dtype=torch.float64, device=device,
+                      generator=torch.Generator(device=device).manual_seed(args.seed))
+    forms = {
+        "fp32": (ProjectionSpec(args.samples, active_volume=True, precision="float32",
+                                sampling_precision="float32"), torch.float32),
+        "fp64": (ProjectionSpec(args.samples, active_volume=True, precision="float64",
+                                sampling_precision="float64"), torch.float64),
+        "cell_gauss_fp64": (ProjectionSpec(args.samples, active_volume=True, precision="float64",
+                                           sampling_precision="float64", integration="cell_gauss"), torch.float64),
+    }
+    fullscan = {}
+    realised = None
+    for name, (spec, out_dtype) in forms.items():
+        ws = ProjectionWorkspace(plan, spec, device)
+        if realised is None:
+            lower, upper, _ = ws.counts(poses)
+            realised = int((upper > lower).sum()) * args.samples
+        seed = cot.to(spec.image_dtype)
+        volume_dtype = torch.float32 if name == "fp32" else torch.float64
+        moments = ws.moments_preferred()
+
+        def iteration():
+            ws.forward(values, poses, moments=moments)
+            ws.vjp(values, poses, seed, volume=True, pose="tangent", volume_dtype=volume_dtype)
+
+        row = {"forward_ms": timed(lambda: ws.forward(values, poses)),
+               "volume_vjp_ms": timed(lambda: ws.vjp(values, poses, seed, volume=True, pose=None,
+                                                     volume_dtype=volume_dtype)),
+               "pose_vjp_ms": timed(lambda: ws.vjp(values, poses, seed, volume=False, pose="tangent")),
+               "iteration_ms": timed(iteration)}
+        if spec.integration == "midpoint":
+            row["iteration_realised_samples_per_s"] = round(realised / (row["iteration_ms"] * 1e-3), 1)
+        fullscan[name] = row
+        del ws
+        torch.cuda.empty_cache()
+
+    # ---- native chest stand-in
+    shape = (139, 512, 512)
+    chest_spacing = (0.7617, 0.7617, 2.5)
+    chest_grid = centred_grid(shape, chest_spacing)
+    diagonal = math.sqrt(sum((n * h) ** 2 for n, h in zip(shape[::-1], chest_spacing, strict=True)))
+    sod, sdd = max(1000.0, 2.0 * diagonal), max(1500.0, 3.0 * diagonal)
+    width = 1.05 * diagonal * sdd / (sod - diagonal / 2.0)
+    chest_geometry = ConeBeamIntrinsics(sod, sdd, (512, 512), (width / 512, width / 512)).batch(
+        (math.pi, math.pi / 2.0, 3.0 * math.pi / 4.0))
+    chest_plan = plan_rays(chest_grid, chest_geometry)
+    chest_values = torch.tensor(chest_phantom(chest_grid, seed=args.seed), device=device)
+    chest_poses = identity(3)
+    native = {}
+    for mode in ("float64", "mixed_float32", "fast_float32"):
+        ws = ProjectionWorkspace(chest_plan, ProjectionSpec(args.samples, active_pose=False, precision="float64",
+                                                            sampling_precision=mode), device)
+        native[mode] = {"forward_ms": timed(lambda: ws.forward(chest_values, chest_poses))}
+        del ws
+    print(json.dumps({
+        "metric": "per-operation device time (median of --steps launches)", "unit": "ms",
+        "fullscan": {"config": {"workload": f"{args.size}^3 chest at {spacing} mm, {args.views} views "
+                                            f"{args.detector}^2, S={args.samples}",
+                                "realised_ray_samples": realised,
+                                "nominal_ray_samples": args.views * args.detector ** 2 * args.samples},
+                     "results": fullscan},
+        "native_chest": {"config": {"workload": "synthetic chest on 512x512x139 at 0.7617x0.7617x2.5 mm, "
+                                                f"3 views 512^2, S={args.samples}, FP64 output",
+                                    "sod_mm": round(sod, 3), "sdd_mm": round(sdd, 3),
+                                    "detector_pitch_mm": round(width / 512, 5)},
+                         "results": native},
+        "data": "synthetic", "steps": args.steps}), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -938,6 +1059,8 @@ def main() -> None:
         run_gather(args)
     elif args.mode == "panels":
         run_panels(args)
+    elif args.mode == "table":
+        run_table(args)
     else:
         run_gpu(args)
 

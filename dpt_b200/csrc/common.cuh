@@ -525,6 +525,23 @@ struct CellCache {
     }
 };
 
+// The current cell's eight corner values widened to FP64 once per cell.
+template <class Field>
+struct WideCellCache {
+    double v[8];
+    int cell = -1;
+    __device__ __forceinline__ void fetch(const Field& f, int lx, int ly, int lz, int index)
+    {
+        if (index != cell) {
+            float narrow[8];
+            f.load_at(index, lx, ly, lz, narrow);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) v[c] = (double)narrow[c];
+            cell = index;
+        }
+    }
+};
+
 // Axis coordinate of a point known to satisfy 0 <= p < n-1 (the interior of the grid): the
 // clamp and the cap of axis32 are then no-ops, so this is the same lower cell and fraction.
 __device__ __forceinline__ Axis32 interior_axis(float p)

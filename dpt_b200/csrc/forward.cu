@@ -215,7 +215,9 @@ __global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, O
                     y = fmaf(offset, sv[1], entry[1]);
                     z = fmaf(offset, sv[2], entry[2]);
                 };
-                CellCache<Field> cache;
+                // MIXED keeps the cell's corners widened to FP64, so a sample widens only its
+                // eight weights (the products w_c v_c are exact in FP64 either way)
+                std::conditional_t<kArith == DPT_ARITH_FAST, CellCache<Field>, WideCellCache<Field>> cache;
                 auto add = [&](Axis32 X, Axis32 Y, Axis32 Z) {
                     cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * dims.ny + Y.lower) * dims.nx + X.lower);
                     float w[8];
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, O
                     } else {
                         double value = 0.0;
 #pragma unroll
-                        for (int c = 0; c < 8; ++c) value = fma((double)w[c], (double)cache.v[c], value);
+                        for (int c = 0; c < 8; ++c) value = fma((double)w[c], cache.v[c], value);
                         integral = integral + value;
                     }
                 };
@@ -311,17 +313,14 @@ __global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, O
                     }, first, last);
                     const double mx = (double)(a.grid.nx - 1), my = (double)(a.grid.ny - 1), mz = (double)(a.grid.nz - 1);
                     const int cx = max(a.grid.nx - 2, 0), cy = max(a.grid.ny - 2, 0), cz = max(a.grid.nz - 2, 0);
-                    CellCache<Field> cache;
+                    WideCellCache<Field> cache;
 #pragma unroll 2
                     for (int i = first; i <= last; ++i) {
                         double p[3];
                         at(i, p);
                         const Axis64 X = axis64(p[0], mx, cx), Y = axis64(p[1], my, cy), Z = axis64(p[2], mz, cz);
                         cache.fetch(f, X.lower, Y.lower, Z.lower, (Z.lower * a.grid.ny + Y.lower) * a.grid.nx + X.lower);
-                        double v[8];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) v[c] = (double)cache.v[c];
-                        integral = integral + interpolate64(X.fraction, Y.fraction, Z.fraction, v);
+                        integral = integral + interpolate64(X.fraction, Y.fraction, Z.fraction, cache.v);
                     }
                     if (last < S - 1) integral = integral + 0.0;
                 }
