@@ -60,6 +60,7 @@ EXPORTS = (
     "dpt_b200_objective_check",
     "dpt_b200_objective",
     "dpt_b200_reduce_sum",
+    "dpt_b200_read_probe",
 )
 
 
@@ -139,6 +140,7 @@ _SIGNATURES = {
     "dpt_b200_objective": (
         [_V, _I, _I, _V, _V, _V, _L, _I, _D, _D, _V, _V, _V, _V, _V], ctypes.c_int),
     "dpt_b200_reduce_sum": ([_V, _L, _V, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_read_probe": ([_V, _L, _I, _V, _V], ctypes.c_int),
 }
 
 _lock = threading.Lock()

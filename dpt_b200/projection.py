@@ -493,7 +493,7 @@ class ProjectionWorkspace:
                 size = lib.dpt_b200_moments_bytes(self.problem, self.views)
                 if self._moments is None or self._moments.numel() * 4 < size:
                     self._moments = torch.empty(size // 4, dtype=torch.float32, device=self.device)
-                self._run("forward", lambda: lib.dpt_b200_forward_moments(
+                self._run("forward_moments", lambda: lib.dpt_b200_forward_moments(
                     self.problem, self.rays(poses), packed.data_ptr(), out.data_ptr(),
                     self._moments.data_ptr(), self.status.data_ptr(), _stream(self.device)))
                 self._moments_for = (field, poses, field._version, poses._version)
@@ -542,6 +542,8 @@ class ProjectionWorkspace:
             batch = self.spec.batch_views if volume else self.views
             rays_per_view = self.plan.rays_per_view
             element = cot.element_size()
+            # launch-log label: what each sampling launch computes
+            label = "vjp" if (volume and components and not split) else "vjp_volume" if volume else "vjp_pose"
             if split:
                 self._run("pose_from_moments", lambda: lib.dpt_b200_pose_from_moments(
                     self.problem, self.rays(poses), self._moments.data_ptr(), cot.data_ptr(),
@@ -554,7 +556,7 @@ class ProjectionWorkspace:
                 if partials is not None and not split:
                     tiles = lib.dpt_b200_pose_partials_bytes(self.problem, 1) // (12 * 8)
                     part_ptr = partials.data_ptr() + first * tiles * components * 8
-                self._run("vjp", lambda: lib.dpt_b200_vjp(self.problem, self.rays(poses, first, count), packed.data_ptr(),
+                self._run(label, lambda: lib.dpt_b200_vjp(self.problem, self.rays(poses, first, count), packed.data_ptr(),
                                      seed_ptr, flags, accumulator, part_ptr, self.status.data_ptr(),
                                      stream), first, count)
                 if volume:

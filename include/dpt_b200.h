@@ -382,6 +382,14 @@ int dpt_b200_objective(const void* prediction, int32_t prediction_dtype, int32_t
 int dpt_b200_reduce_sum(const double* values, int64_t count, double* scratch, double* total,
                         int32_t* status, void* stream);
 
+/* ---- measurement --------------------------------------------------------------------
+ * No reference counterpart: the roofline the benchmark reports for the gather kernels.
+ * Reads `bytes` (a multiple of 16) from the 16-byte aligned device `buffer` `passes` times
+ * in one launch (no writes; `sink` is one device float that is written only if the
+ * buffer's sum is NaN).  Bandwidth = passes * bytes / launch time; for a buffer that fits
+ * in L2 this is the L2 read rate of the device. */
+int dpt_b200_read_probe(const void* buffer, int64_t bytes, int32_t passes, float* sink, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -142,3 +142,13 @@ def test_null_pointers_and_view_ranges_are_rejected():
     assert lib.dpt_b200_finish_pose(p, 2, 3, 12, 16, 16, 0, 16, None) == -5
     assert lib.dpt_b200_fold_volume(p, 32, None, 0, None, N.F32, 1, 16, None) == -1
     assert lib.dpt_b200_error_string(-5) == b"view range outside the problem"
+
+
+def test_read_probe_rejects_bad_buffers_without_launching():
+    lib = N.library()
+    assert lib.dpt_b200_read_probe(None, 16, 1, 16, None) == -1
+    assert lib.dpt_b200_read_probe(16, 16, 1, None, None) == -1
+    assert lib.dpt_b200_read_probe(16, 24, 1, 16, None) == -2  # not a multiple of 16 bytes
+    assert lib.dpt_b200_read_probe(16, 0, 1, 16, None) == -2
+    assert lib.dpt_b200_read_probe(16, 16, 0, 16, None) == -2
+    assert lib.dpt_b200_read_probe(24, 16, 1, 16, None) == -6  # buffer not 16-byte aligned
