@@ -35,6 +35,11 @@
 #ifndef DPT_VJP_MIN_BLOCKS_F32C
 #define DPT_VJP_MIN_BLOCKS_F32C 8
 #endif
+// FP32 pose moments: alpha_i = (i + 0.5) / S as one multiplication by 1/S when S is a power
+// of two (both exact), else from a per-block table of IEEE quotients
+#ifndef DPT_VJP_POW2_ALPHA
+#define DPT_VJP_POW2_ALPHA 1
+#endif
 // The compensated form's forward that stores the pose moments (no scatter) measured 158.6 ->
 // 153.4 ms per 360-view full scan at nine blocks (56 registers), 155.4 at ten.
 #ifndef DPT_VJP_MIN_BLOCKS_F32C_FORWARD
@@ -202,13 +207,14 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                     int pending = -1;
                     CellCache<Field, kVjpReuse> cache;
                     auto position_at = [&](int i) { return fmaf((float)i + 0.5f, step, iv.lower); };
+                    const float inverse_samples = 1.0f / (float)S;
                     // One midpoint.  mode 0: general (support and finiteness tested); 1: on the
                     // inside run (both known to pass); 2: on the interior run (no clamp active,
                     // slope masks 1).
                     // `bounded` (every increment finite and at most 1 in magnitude) is fixed
                     // per ray: the march is instantiated for both values so the sample loop
                     // carries no test of it
-                    auto visit = [&](int i, int mode, auto bounded_tag) {
+                    auto visit = [&](int i, int mode, auto bounded_tag, auto pow2_tag) {
                         constexpr bool kBounded = decltype(bounded_tag)::value;
                         const bool known_inside = mode > 0;
                         const float position = position_at(i);
@@ -253,7 +259,13 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                 dO[k] = dO[k] + gs[k];
                                 dD[k] = fmaf(position, gs[k], dD[k]);
                             }
-                            const float alpha = i < kAlphaTable ? alpha_table[i] : ((float)i + 0.5f) / (float)S;
+                            // S a power of two: (i + 0.5) / S is exact, and so is the product
+                            // with the exact reciprocal
+                            float alpha;
+                            if constexpr (decltype(pow2_tag)::value)
+                                alpha = ((float)i + 0.5f) * inverse_samples;
+                            else
+                                alpha = i < kAlphaTable ? alpha_table[i] : ((float)i + 0.5f) / (float)S;
                             const float along = fmaf(gs[2], d[2], fmaf(gs[1], d[1], gs[0] * d[0]));
                             sl = fmaf(1.0f - alpha, along, sl);
                             su = fmaf(alpha, along, su);
@@ -296,9 +308,9 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                             }
                         }
                     };
-                    auto march = [&](auto bounded_tag) {
+                    auto march = [&](auto bounded_tag, auto pow2_tag) {
                     if (!moderate(o, d)) {
-                        for (int i = 0; i < S; ++i) visit(i, 0, bounded_tag);
+                        for (int i = 0; i < S; ++i) visit(i, 0, bounded_tag, pow2_tag);
                     } else {
                         // samples outside the inside run add exact zeros to every moment
                         int first, last;
@@ -315,10 +327,10 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                             return x >= 0.0f && x < dims.mx && y >= 0.0f && y < dims.my && z >= 0.0f && z < dims.mz;
                         }, ifirst, ilast);
                         const int split = min(ifirst, last + 1);
-                        for (int i = first; i < split; ++i) visit(i, 1, bounded_tag);
+                        for (int i = first; i < split; ++i) visit(i, 1, bounded_tag, pow2_tag);
 #pragma unroll 2
-                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2, bounded_tag);
-                        for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1, bounded_tag);
+                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2, bounded_tag, pow2_tag);
+                        for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1, bounded_tag, pow2_tag);
                         trailing_zero = last < S - 1;
                     }
                     };
@@ -332,10 +344,22 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                         }
                         sl = m[7 * ma.stride];
                         su = m[8 * ma.stride];
-                    } else if (bounded) {
-                        march(std::true_type{});
                     } else {
-                        march(std::false_type{});
+                        // the pose moments' alpha_i by one multiplication when S is a power of two
+                        auto run = [&](auto bounded_tag) {
+                            if constexpr (kPose && DPT_VJP_POW2_ALPHA != 0) {
+                                if ((S & (S - 1)) == 0)
+                                    march(bounded_tag, std::true_type{});
+                                else
+                                    march(bounded_tag, std::false_type{});
+                            } else {
+                                march(bounded_tag, std::false_type{});
+                            }
+                        };
+                        if (bounded)
+                            run(std::true_type{});
+                        else
+                            run(std::false_type{});
                     }
                     if (kVol && pending >= 0) flush_cell(acc, pending, cs);
                     if constexpr (kMoments == kStoreMoments) {
