@@ -484,6 +484,14 @@ __device__ __forceinline__ bool moderate(const float* o, const float* d)
                           fmaxf(fabsf(d[1]), fabsf(d[2])));
     return m < 1e30f;
 }
+// The compensated form walks cell runs (segment form) while a ray's samples lie at most one
+// cell plane apart on average, (|s_x| + |s_y|) + |s_z| <= 1 for the per-sample step s in grid
+// units; sparser samples take the per-sample form (walking every plane between them costs
+// more than evaluating each sample), as do rays whose coordinates reach 1e30.
+__device__ __forceinline__ bool segment_form(const float* entry, const float* sv)
+{
+    return moderate(entry, sv) && (fabsf(sv[0]) + fabsf(sv[1])) + fabsf(sv[2]) <= 1.0f;
+}
 __device__ __forceinline__ bool moderate(const double* o, const double* d)
 {
     const double m = fmax(fmax(fmax(fabs(o[0]), fabs(o[1])), fmax(fabs(o[2]), fabs(d[0]))),

@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, O
                     z = fmaf(offset, sv[2], entry[2]);
                 };
                 double total;
-                if (!moderate(entry, sv)) {
+                if (!segment_form(entry, sv)) {
                     // per-sample form: polynomial samples, blocked compensated sum
                     BlockSum acc;
                     PolyCache<Field> cache;

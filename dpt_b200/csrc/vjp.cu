@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                     if constexpr (kMoments == kLoadMoments) {
 #pragma unroll
                         for (int k = 0; k < kMomentWords; ++k) words[k] = ma.moments[k * ma.stride + ray_index];
-                    } else if (moderate(entry, sv)) {
+                    } else if (segment_form(entry, sv)) {
                         // segment form: every cell run in closed form
                         int first, last;
                         inside_run(S, [&](int i) {
@@ -851,7 +851,8 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                             words[5 + k] = Hs[k];
                         }
                     } else {
-                        // per-sample form (rays reaching 1e30 in grid coordinates)
+                        // per-sample form (samples more than a cell plane apart, or rays
+                        // reaching 1e30 in grid coordinates)
                         const float inv_s = 1.0f / (float)S;
                         BlockSum mean;
                         float G[3] = {0.0f, 0.0f, 0.0f}, H[3] = {0.0f, 0.0f, 0.0f};

@@ -531,7 +531,8 @@ static void point32c(const float* entry, const float* step_vector, int index, fl
  * half-cell margin, where the fraction is clamped), so the run's sum of the cell polynomial,
  * its slope sums and the volume moments are polynomials in j of degree <= 3, evaluated in
  * closed form with the power sums S1 = sum j, S2 = sum j^2, S3 = sum j^3.  Rays whose grid
- * origin or direction reach 1e30 take the per-sample form instead. */
+ * origin or direction reach 1e30, or whose samples lie more than one cell plane apart on
+ * average, take the per-sample form instead. */
 
 static int moderate32c(const float* entry, const float* step_vector)
 {
@@ -541,6 +542,15 @@ static int moderate32c(const float* entry, const float* step_vector)
         m = fmaxf(m, fabsf(step_vector[a]));
     }
     return m < 1e30f;
+}
+
+/* Segment form while the samples lie at most one cell plane apart on average,
+ * (|s_x| + |s_y|) + |s_z| <= 1 (this library's rule; sparser samples take the per-sample
+ * form, whose sums round differently). */
+static int segment_form32c(const float* entry, const float* step_vector)
+{
+    const float planes = (fabsf(step_vector[0]) + fabsf(step_vector[1])) + fabsf(step_vector[2]);
+    return moderate32c(entry, step_vector) && planes <= 1.0f;
 }
 
 /* First and last samples inside the support (first > last when none): the points are
@@ -1106,7 +1116,7 @@ static int forward_ray(const dpt_problem* p, const void* field, const ray_t* ray
             float entry[3], stepv[3];
             march32c(ray, S, entry, stepv);
             double total;
-            if (moderate32c(entry, stepv)) {
+            if (segment_form32c(entry, stepv)) {
                 int first, last;
                 inside_run32c(entry, stepv, shape, S, &first, &last);
                 fwd_context32c ctx = {p, field, {0.0f, 0.0f}};
@@ -1693,7 +1703,7 @@ static int vjp_ray_f32c(const dpt_problem* p, const void* field, const ray_t* ra
     float volume_factor = (float)(seed * ray->r.length * step);
     float entry[3], stepv[3];
     march32c(ray, S, entry, stepv);
-    if (moderate32c(entry, stepv)) {
+    if (segment_form32c(entry, stepv)) {
         int first, last;
         inside_run32c(entry, stepv, shape, S, &first, &last);
         vjp_context32c ctx;
