@@ -272,6 +272,21 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                         }
                         if (kVol) {
                             if (in) {
+                                if constexpr (kBounded) {
+                                    // a run's first increments start its sums (0 + x differs
+                                    // from x only for x = -0, and a -0 run sum leaves the
+                                    // +0-initialised accumulator slot exactly as +0 does):
+                                    // 234.8 ms per full-scan volume pass, 235.9 with zeroing
+                                    if (cell != pending) {
+                                        if (pending >= 0) flush_cell(acc, pending, cs);
+                                        pending = cell;
+#pragma unroll
+                                        for (int c = 0; c < 8; ++c) cs[c] = mul_ftz(vf, w[c]);
+                                    } else {
+#pragma unroll
+                                        for (int c = 0; c < 8; ++c) cs[c] = cs[c] + mul_ftz(vf, w[c]);
+                                    }
+                                } else {
                                 if (cell != pending) {
                                     if (pending >= 0) flush_cell(acc, pending, cs);
 #pragma unroll
@@ -299,6 +314,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                             }
                                         }
                                     }
+                                }
                                 }
                             } else if (pending >= 0) {
                                 flush_cell(acc, pending, cs);
