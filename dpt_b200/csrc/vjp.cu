@@ -287,16 +287,14 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                         for (int c = 0; c < 8; ++c) cs[c] = cs[c] + mul_ftz(vf, w[c]);
                                     }
                                 } else {
-                                if (cell != pending) {
-                                    if (pending >= 0) flush_cell(acc, pending, cs);
+                                    // increments that may be non-finite or large: each one is
+                                    // checked, and a sum that would overflow is flushed first
+                                    if (cell != pending) {
+                                        if (pending >= 0) flush_cell(acc, pending, cs);
 #pragma unroll
-                                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
-                                    pending = cell;
-                                }
-                                if constexpr (kBounded) {
-#pragma unroll
-                                    for (int c = 0; c < 8; ++c) cs[c] = cs[c] + mul_ftz(vf, w[c]);
-                                } else {
+                                        for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
+                                        pending = cell;
+                                    }
                                     float* slot = acc + 8 * (int64_t)cell;
 #pragma unroll
                                     for (int c = 0; c < 8; ++c) {
@@ -314,7 +312,6 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                             }
                                         }
                                     }
-                                }
                                 }
                             } else if (pending >= 0) {
                                 flush_cell(acc, pending, cs);
