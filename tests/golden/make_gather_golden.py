@@ -1,8 +1,8 @@
 """Generate ``gather.npz`` / ``gather.json``: the scenes of the reference's deterministic-gather
-tests and their independent FP64 midpoint matrices.  Run in a checkout that has the reference
-project at ``/root/reference`` (its host code imports without Warp):
+tests and their independent FP64 midpoint matrices.  Run with the reference checkout given
+by ``--reference PATH`` or ``DPT_REFERENCE`` (its host code imports without Warp):
 
-    python tests/golden/make_gather_golden.py
+    python tests/golden/make_gather_golden.py --reference PATH
 
 Sources used (paths inside the reference project):
   * tests/python/warp_cpu/test_projection_adjoint_gather.py:26-74 ``_metadata`` (scenes
@@ -26,9 +26,12 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE = Path("/root/reference")
 HERE = Path(__file__).resolve().parent
-sys.path.insert(0, str(REFERENCE / "python"))
+sys.path.insert(0, str(HERE))
+
+from reference_checkout import reference_root  # noqa: E402
+
+REFERENCE = reference_root()
 
 from dpt import geometry as rg  # noqa: E402
 from dpt.validation import projection as rv  # noqa: E402

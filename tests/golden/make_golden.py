@@ -1,8 +1,8 @@
 """Generate the golden fixtures in this directory from the reference projector's own
-pure-Python oracles.  Run in a checkout that has the reference project at
-``/root/reference`` (its host code imports without Warp):
+pure-Python oracles.  Run with the reference checkout given by ``--reference PATH`` or
+``DPT_REFERENCE`` (its host code imports without Warp):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference PATH
 
 Sources used (paths inside the reference project):
   * python/dpt/validation/projection.py   - FP64 midpoint / exact piecewise-Gauss integrals
@@ -30,10 +30,12 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE = Path("/root/reference")
 HERE = Path(__file__).resolve().parent
-sys.path.insert(0, str(REFERENCE / "python"))
-sys.path.insert(0, str(REFERENCE))
+sys.path.insert(0, str(HERE))
+
+from reference_checkout import reference_root  # noqa: E402
+
+REFERENCE = reference_root()
 
 from dpt import geometry as rg  # noqa: E402
 from dpt import phantoms as rp  # noqa: E402

@@ -1,8 +1,8 @@
 """Generate ``pointwise.npz``: golden vectors of the transmission and objective operators from
-the reference project's own exact-input Decimal oracles.  Run in a checkout that has the
-reference project at ``/root/reference`` (these modules import without Warp):
+the reference project's own exact-input Decimal oracles.  Run with the reference checkout
+given by ``--reference PATH`` or ``DPT_REFERENCE`` (these modules import without Warp):
 
-    python tests/golden/make_pointwise_golden.py
+    python tests/golden/make_pointwise_golden.py --reference PATH
 
 Sources used (paths inside the reference project):
   * python/dpt/validation/transmission.py - forward_reference, inverse_reference,
@@ -20,9 +20,12 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE = Path("/root/reference")
 HERE = Path(__file__).resolve().parent
-sys.path.insert(0, str(REFERENCE / "python"))
+sys.path.insert(0, str(HERE))
+
+from reference_checkout import reference_root  # noqa: E402
+
+REFERENCE = reference_root()
 
 from dpt.validation import objectives as ro  # noqa: E402
 from dpt.validation import transmission as rt  # noqa: E402
