@@ -46,6 +46,7 @@ RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status, 
     a.block_cols = tile_cols(p, threads);
     a.block_rows = threads / a.block_cols;
     a.warps_x = a.block_cols / 8;
+    a.view_group = DPT_VIEW_GROUP;
     a.poses = r.poses;
     a.view_table = r.view_table;
     a.ray_sources = r.ray_sources;
@@ -59,7 +60,7 @@ RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status, 
 namespace {
 
 constexpr int64_t kMaxIndex = 2147483647;  // signed 32-bit indexing, as the reference
-constexpr int kMaxViewsPerLaunch = 65535;   // gridDim.y limit
+constexpr int kMaxViewsPerLaunch = 65535;   // views per launch of the ray kernels
 
 bool aligned(const void* p, uintptr_t bytes) { return (reinterpret_cast<uintptr_t>(p) % bytes) == 0; }
 
@@ -106,15 +107,19 @@ int check_rays(const dpt_problem* p, const dpt_rays* r)
 
 int to_code(cudaError_t e) { return e == cudaSuccess ? DPT_OK : (int)e; }
 
-// Launch `body` on chunks of at most kMaxViewsPerLaunch views.
+// Launch `body` on chunks of at most kMaxViewsPerLaunch views, and few enough that the 1-D
+// grid of views x tiles stays below 2^31 blocks.
 template <typename Body>
 int chunked(const dpt_problem* p, const dpt_rays* r, int32_t* status, int threads, Body body)
 {
-    for (int32_t first = 0; first < r->view_count; first += kMaxViewsPerLaunch) {
+    int tiles_x;
+    const int64_t tiles = dpt::tiles_per_view(*p, &tiles_x, threads);
+    const int64_t by_grid = ((int64_t)1 << 31) / (tiles > 0 ? tiles : 1) - 1;
+    const int32_t most = (int32_t)(by_grid < kMaxViewsPerLaunch ? (by_grid < 1 ? 1 : by_grid) : kMaxViewsPerLaunch);
+    for (int32_t first = 0; first < r->view_count; first += most) {
         dpt_rays part = *r;
         part.view_begin = r->view_begin + first;
-        part.view_count = r->view_count - first < kMaxViewsPerLaunch ? r->view_count - first
-                                                                      : kMaxViewsPerLaunch;
+        part.view_count = r->view_count - first < most ? r->view_count - first : most;
         const dpt::RayArgs a = dpt::make_ray_args(*p, part, status, threads);
         const int code = body(a, first);
         if (code != DPT_OK) return code;

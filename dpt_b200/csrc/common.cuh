@@ -53,6 +53,7 @@ struct RayArgs {
     int block_rows;      // detector rows per block tile: block_threads / block_cols
     int warps_x;         // warps along the columns of a block tile: block_cols / 8
     int block_threads;   // threads per block
+    int view_group;      // views per block-order group (see block_work)
     const double* poses;       // absolute view indexing
     const double* view_table;  // absolute view indexing
     const double* ray_sources;
@@ -101,6 +102,36 @@ __device__ __forceinline__ bool rigid_pose(const double* p)
                        p[2] * (p[3] * p[7] - p[4] * p[6]);
     if (det < 0.0) valid = false;
     return valid;
+}
+
+// Views per group of the block order of the ray kernels.  The 1-D grid walks groups of
+// view_group consecutive views; inside a group the blocks of one detector tile for all of the
+// group's views are consecutive.  The blocks resident at one time then cover a few tiles of
+// several neighbouring views, whose rays cross nearly the same cells: the field copy and the
+// volume accumulator records they touch are shared in L2 instead of each view streaming the
+// whole volume through it (a launch's blocks are dispatched roughly in index order).
+#ifndef DPT_VIEW_GROUP
+#define DPT_VIEW_GROUP 8
+#endif
+
+// Blocks of a launch over a.views views and a.tiles_per_view tiles per view.
+__host__ __device__ __forceinline__ unsigned ray_blocks(const RayArgs& a)
+{
+    return (unsigned)a.tiles_per_view * (unsigned)a.views;
+}
+
+// (view within the launch, detector tile) of this block.
+__device__ __forceinline__ void block_work(const RayArgs& a, int* view_local, int* tile)
+{
+    const int b = (int)blockIdx.x;
+    const int per_group = a.view_group * a.tiles_per_view;
+    const int g = b / per_group;
+    const int r = b - g * per_group;
+    const int first = g * a.view_group;
+    const int views = min(a.view_group, a.views - first);
+    const int t = r / views;
+    *tile = t;
+    *view_local = first + (r - t * views);
 }
 
 // Ray index inside its view -> (pixel) for the tiled panel mapping, or the bundle index.
@@ -466,12 +497,14 @@ struct FieldDims {
     float hx, hy, hz;   // n - 0.5: upper end of the half-cell support
     float mx, my, mz;   // n - 1: clamp bound
     int cx, cy, cz;     // max(n - 2, 0): largest lower cell index
+    bool packed;        // interior coordinates stay below 2^23 (interior_fraction2 applies)
     __device__ __forceinline__ void init(const Grid& g)
     {
         nx = g.nx; ny = g.ny; nz = g.nz;
         hx = (float)nx - 0.5f; hy = (float)ny - 0.5f; hz = (float)nz - 0.5f;
         mx = (float)(nx - 1); my = (float)(ny - 1); mz = (float)(nz - 1);
         cx = max(nx - 2, 0); cy = max(ny - 2, 0); cz = max(nz - 2, 0);
+        packed = nx <= (1 << 23) && ny <= (1 << 23) && nz <= (1 << 23);
     }
 };
 
@@ -946,6 +979,120 @@ __device__ __forceinline__ float mul_ftz(float a, float b)
     float r;
     asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
     return r;
+}
+
+// ------------------------------------------------------------ packed FP32 pairs
+//
+// sm_100 executes add/sub/mul/fma on two FP32 lanes held in one 64-bit register pair per
+// instruction, each lane rounded exactly as the scalar instruction rounds it.  The FP32
+// sample loops evaluate two consecutive samples of a ray per instruction wherever their
+// arithmetic is lane-wise (positions, coordinates, floors, corner weights, slopes, scatter
+// increments): half the issue slots for the same results bit for bit.  Serial sums (the ray
+// sum, the moments, a cell run's corner sums) stay scalar, sample i before sample i + 1.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pack2(float lo, float hi)
+{
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ f32x2 splat2(float v) { return pack2(v, v); }
+__device__ __forceinline__ float lo2(f32x2 v)
+{
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return a;
+}
+__device__ __forceinline__ float hi2(f32x2 v)
+{
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return b;
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+// lane-wise mul_ftz: results below the normal range flushed to signed zero
+__device__ __forceinline__ f32x2 mul_ftz2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c)
+{
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// Floor of two coordinates known to satisfy 0 <= p < 2^23 on the FP32 pipe: p + 2^23 rounded
+// toward -inf is 2^23 + floor(p) exactly (the sum lies in [2^23, 2^24), where the floats are
+// the integers), so its bit pattern is 0x4B000000 + floor(p) and subtracting 2^23 again gives
+// floor(p) exactly.  The fraction p - floor(p) is exact (Sterbenz), so this equals
+// interior_axis lane by lane.  Returns the fractions; `biased` receives the biased floors.
+constexpr float kFloorMagic = 8388608.0f;  // 2^23
+constexpr int kFloorBias = 0x4B000000;     // bit pattern of 2^23
+__device__ __forceinline__ f32x2 interior_fraction2(f32x2 p, f32x2* biased)
+{
+    f32x2 t;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(t) : "l"(p), "l"(splat2(kFloorMagic)));
+    *biased = t;
+    return sub2(p, sub2(t, splat2(kFloorMagic)));
+}
+__device__ __forceinline__ int biased_lo(f32x2 t) { return __float_as_int(lo2(t)) - kFloorBias; }
+__device__ __forceinline__ int biased_hi(f32x2 t) { return __float_as_int(hi2(t)) - kFloorBias; }
+
+// Trilinear corner weights of two samples, (f0 f1) f2 per lane (corner_weights lane-wise).
+__device__ __forceinline__ void corner_weights2(f32x2 fx, f32x2 fy, f32x2 fz, f32x2* w, f32x2* ax_out = nullptr,
+                                                f32x2* ay_out = nullptr, f32x2* az_out = nullptr)
+{
+    const f32x2 one = splat2(1.0f);
+    const f32x2 ax = sub2(one, fx), ay = sub2(one, fy), az = sub2(one, fz);
+    const f32x2 p00 = mul2(ax, ay), p10 = mul2(fx, ay), p01 = mul2(ax, fy), p11 = mul2(fx, fy);
+    w[0] = mul2(p00, az);
+    w[1] = mul2(p10, az);
+    w[2] = mul2(p01, az);
+    w[3] = mul2(p11, az);
+    w[4] = mul2(p00, fz);
+    w[5] = mul2(p10, fz);
+    w[6] = mul2(p01, fz);
+    w[7] = mul2(p11, fz);
+    if (ax_out) *ax_out = ax;
+    if (ay_out) *ay_out = ay;
+    if (az_out) *az_out = az;
+}
+
+// Interior slopes of two samples (slope32 with every mask 1), from each sample's eight corner
+// values: the twelve differences per sample are scalar, their combination lane-wise.
+__device__ __forceinline__ void slope2(f32x2 fx, f32x2 fy, f32x2 fz, f32x2 ax, f32x2 ay, f32x2 az,
+                                       const float* u, const float* v, f32x2* g)
+{
+    const f32x2 d10 = pack2(u[1] - u[0], v[1] - v[0]), d32 = pack2(u[3] - u[2], v[3] - v[2]);
+    const f32x2 d54 = pack2(u[5] - u[4], v[5] - v[4]), d76 = pack2(u[7] - u[6], v[7] - v[6]);
+    g[0] = fma2(fz, fma2(fy, d76, mul2(ay, d54)), mul2(az, fma2(fy, d32, mul2(ay, d10))));
+    const f32x2 d20 = pack2(u[2] - u[0], v[2] - v[0]), d31 = pack2(u[3] - u[1], v[3] - v[1]);
+    const f32x2 d64 = pack2(u[6] - u[4], v[6] - v[4]), d75 = pack2(u[7] - u[5], v[7] - v[5]);
+    g[1] = fma2(fz, fma2(fx, d75, mul2(ax, d64)), mul2(az, fma2(fx, d31, mul2(ax, d20))));
+    const f32x2 d40 = pack2(u[4] - u[0], v[4] - v[0]), d51 = pack2(u[5] - u[1], v[5] - v[1]);
+    const f32x2 d62 = pack2(u[6] - u[2], v[6] - v[2]), d73 = pack2(u[7] - u[3], v[7] - v[3]);
+    g[2] = fma2(fy, fma2(fx, d73, mul2(ax, d62)), mul2(ay, fma2(fx, d51, mul2(ax, d40))));
 }
 
 // Per-block staging of the view's pose (12 doubles) and panel record.

@@ -2,8 +2,8 @@
 //
 // One thread marches one ray; a 128-thread block covers a 16x8 detector tile (each warp
 // an 8x4 sub-tile) so the 32 rays of a warp sample neighbouring voxels at every step and
-// their corner loads share L1 lines.  One launch covers every view of a call (blockIdx.y
-// is the view), where the reference launches once per view.
+// their corner loads share L1 lines.  One launch covers every view of a call, where the
+// reference launches once per view; the blocks run in groups of neighbouring views (block_work).
 //
 // Arithmetic per mode (reference hcltech-robotics/dpt):
 //   F32  - python/dpt/kernels/projection_fp32.py:334-374 (FP64 setup, FP32 clip, fmaf
@@ -65,11 +65,12 @@ template <int kArith, class Field, typename Out>
 __global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, Out* __restrict__ image)
 {
     __shared__ ViewShared vs;
-    const int view_local = blockIdx.y;
+    int view_local, tile;
+    block_work(a, &view_local, &tile);
     const int view = a.view_begin + view_local;
     stage_view(a, view, vs);
     int pixel;
-    if (!ray_of_thread(a, blockIdx.x, &pixel)) return;
+    if (!ray_of_thread(a, tile, &pixel)) return;
 
     double source[3], end[3];
     ray_endpoints(a, vs.table, view, pixel, source, end);
@@ -407,11 +408,12 @@ __global__ void __launch_bounds__(kBlock) k_counts(RayArgs a, double* __restrict
                                                    int32_t* __restrict__ realised)
 {
     __shared__ ViewShared vs;
-    const int view_local = blockIdx.y;
+    int view_local, tile;
+    block_work(a, &view_local, &tile);
     const int view = a.view_begin + view_local;
     stage_view(a, view, vs);
     int pixel;
-    if (!ray_of_thread(a, blockIdx.x, &pixel)) return;
+    if (!ray_of_thread(a, tile, &pixel)) return;
     double source[3], end[3];
     ray_endpoints(a, vs.table, view, pixel, source, end);
     Ray64 r;
@@ -491,7 +493,7 @@ cudaError_t forward_with(const dpt_problem& p, const RayArgs& a, const Field& f,
 cudaError_t launch_forward(const dpt_problem& p, const RayArgs& a, const void* packed, void* image,
                            cudaStream_t stream)
 {
-    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const dim3 grid(ray_blocks(a));
     if (p.arith == DPT_ARITH_F32C && p.layout == DPT_LAYOUT_REPLICATED) {
         PolyF32 f{static_cast<const float4*>(packed), p.nx, p.ny, p.nz};
         return forward_with<DPT_ARITH_F32C>(p, a, f, image, grid, stream);
@@ -515,7 +517,7 @@ cudaError_t launch_forward(const dpt_problem& p, const RayArgs& a, const void* p
 cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower, double* upper,
                           int32_t* realised, cudaStream_t stream)
 {
-    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const dim3 grid(ray_blocks(a));
     if (p.arith == DPT_ARITH_F32)
         k_counts<DPT_ARITH_F32><<<grid, kBlock, 0, stream>>>(a, lower, upper, realised);
     else if (p.arith == DPT_ARITH_F64 || p.arith == DPT_ARITH_CELLS)

@@ -151,7 +151,10 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
     // alpha_i = (i + 0.5) / S of the FP32 pose moments, each one IEEE division, tabulated
     // once per block for the first kAlphaTable samples (later samples divide directly)
     __shared__ float alpha_table[kArith == DPT_ARITH_F32 && kPose && kMoments != kLoadMoments ? kAlphaTable : 1];
-    const int view_local = blockIdx.y;
+    // one cell run's sums into its 32-byte accumulator record
+    auto flush_run = [&](int cell, const float* sums) { flush_cell(acc, cell, sums); };
+    int view_local, tile;
+    block_work(a, &view_local, &tile);
     const int view = a.view_begin + view_local;
     if (kArith == DPT_ARITH_F32 && kPose && kMoments != kLoadMoments) {
         const int n = min(a.samples, kAlphaTable);
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
     }
     stage_view(a, view, vs);
     int pixel;
-    const bool active = ray_of_thread(a, blockIdx.x, &pixel);
+    const bool active = ray_of_thread(a, tile, &pixel);
     const int64_t rays_per_view = (int64_t)a.rows * a.cols;
     const int S = a.samples;
     double g[12];
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                     // +0-initialised accumulator slot exactly as +0 does):
                                     // 234.8 ms per full-scan volume pass, 235.9 with zeroing
                                     if (cell != pending) {
-                                        if (pending >= 0) flush_cell(acc, pending, cs);
+                                        if (pending >= 0) flush_run(pending, cs);
                                         pending = cell;
 #pragma unroll
                                         for (int c = 0; c < 8; ++c) cs[c] = mul_ftz(vf, w[c]);
@@ -290,7 +293,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                     // increments that may be non-finite or large: each one is
                                     // checked, and a sum that would overflow is flushed first
                                     if (cell != pending) {
-                                        if (pending >= 0) flush_cell(acc, pending, cs);
+                                        if (pending >= 0) flush_run(pending, cs);
 #pragma unroll
                                         for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                                         pending = cell;
@@ -314,10 +317,91 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                     }
                                 }
                             } else if (pending >= 0) {
-                                flush_cell(acc, pending, cs);
+                                flush_run(pending, cs);
 #pragma unroll
                                 for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                                 pending = -1;
+                            }
+                        }
+                    };
+                    // Samples i and i + 1 of the interior run, lane-wise where the arithmetic is
+                    // (see "packed FP32 pairs" in common.cuh); the serial sums take sample i,
+                    // then sample i + 1, so every moment, increment and run sum is the value
+                    // the two visits of mode 2 form.  `ip` holds (i + 0.5, i + 1.5).
+                    auto visit_pair = [&](int i, f32x2 ip, auto bounded_tag, auto pow2_tag) {
+                        (void)bounded_tag;
+                        const f32x2 position = fma2(ip, splat2(step), splat2(iv.lower));
+                        const f32x2 x = fma2(position, splat2(d[0]), splat2(o[0]));
+                        const f32x2 y = fma2(position, splat2(d[1]), splat2(o[1]));
+                        const f32x2 z = fma2(position, splat2(d[2]), splat2(o[2]));
+                        f32x2 bx, by, bz;
+                        const f32x2 fx = interior_fraction2(x, &bx);
+                        const f32x2 fy = interior_fraction2(y, &by);
+                        const f32x2 fz = interior_fraction2(z, &bz);
+                        f32x2 w[8], ax, ay, az;
+                        corner_weights2(fx, fy, fz, w, &ax, &ay, &az);
+                        const int lx0 = biased_lo(bx), ly0 = biased_lo(by), lz0 = biased_lo(bz);
+                        const int lx1 = biased_hi(bx), ly1 = biased_hi(by), lz1 = biased_hi(bz);
+                        const int cell0 = (lz0 * dims.ny + ly0) * dims.nx + lx0;
+                        const int cell1 = (lz1 * dims.ny + ly1) * dims.nx + lx1;
+                        if (kPose) {
+                            float u[8], v[8];
+                            f.load_at(cell0, lx0, ly0, lz0, u);
+                            f.load_at(cell1, lx1, ly1, lz1, v);
+                            float wu[8], wv[8];
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) {
+                                wu[c] = lo2(w[c]);
+                                wv[c] = hi2(w[c]);
+                            }
+                            const float value0 = interpolate(wu, u), value1 = interpolate(wv, v);
+                            f32x2 gs[3];
+                            slope2(fx, fy, fz, ax, ay, az, u, v, gs);
+                            mean = mean + value0;
+                            mean = mean + value1;
+                            const float p0 = lo2(position), p1 = hi2(position);
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                dO[k] = dO[k] + lo2(gs[k]);
+                                dO[k] = dO[k] + hi2(gs[k]);
+                                dD[k] = fmaf(p0, lo2(gs[k]), dD[k]);
+                                dD[k] = fmaf(p1, hi2(gs[k]), dD[k]);
+                            }
+                            f32x2 alpha;
+                            if constexpr (decltype(pow2_tag)::value)
+                                alpha = mul2(ip, splat2(inverse_samples));
+                            else
+                                alpha = pack2(i < kAlphaTable ? alpha_table[i] : ((float)i + 0.5f) / (float)S,
+                                              i + 1 < kAlphaTable ? alpha_table[i + 1] : ((float)i + 1.5f) / (float)S);
+                            const f32x2 along = fma2(gs[2], splat2(d[2]), fma2(gs[1], splat2(d[1]), mul2(gs[0], splat2(d[0]))));
+                            const f32x2 rest = sub2(splat2(1.0f), alpha);
+                            sl = fmaf(lo2(rest), lo2(along), sl);
+                            sl = fmaf(hi2(rest), hi2(along), sl);
+                            su = fmaf(lo2(alpha), lo2(along), su);
+                            su = fmaf(hi2(alpha), hi2(along), su);
+                        }
+                        if (kVol) {
+                            // bounded increments only (the pair loop runs for bounded rays)
+                            f32x2 inc[8];
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) inc[c] = mul_ftz2(splat2(vf), w[c]);
+                            if (cell0 != pending) {
+                                if (pending >= 0) flush_run(pending, cs);
+                                pending = cell0;
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) cs[c] = lo2(inc[c]);
+                            } else {
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) cs[c] = cs[c] + lo2(inc[c]);
+                            }
+                            if (cell1 != pending) {
+                                flush_run(pending, cs);
+                                pending = cell1;
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) cs[c] = hi2(inc[c]);
+                            } else {
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) cs[c] = cs[c] + hi2(inc[c]);
                             }
                         }
                     };
@@ -341,8 +425,17 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                         }, ifirst, ilast);
                         const int split = min(ifirst, last + 1);
                         for (int i = first; i < split; ++i) visit(i, 1, bounded_tag, pow2_tag);
-#pragma unroll 2
-                        for (int i = ifirst; i <= ilast; ++i) visit(i, 2, bounded_tag, pow2_tag);
+                        int i = ifirst;
+                        // the pair floors need interior coordinates below 2^23, and the pair
+                        // scatter bounded increments
+                        if (dims.packed && (!kVol || decltype(bounded_tag)::value)) {
+                            f32x2 ip = pack2((float)i + 0.5f, (float)i + 1.5f);
+                            for (; i + 1 <= ilast; i += 2) {
+                                visit_pair(i, ip, bounded_tag, pow2_tag);
+                                ip = add2(ip, splat2(2.0f));
+                            }
+                        }
+                        for (; i <= ilast; ++i) visit(i, 2, bounded_tag, pow2_tag);
                         for (int i = max(ilast + 1, split); i <= last; ++i) visit(i, 1, bounded_tag, pow2_tag);
                         trailing_zero = last < S - 1;
                     }
@@ -374,7 +467,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                         else
                             run(std::false_type{});
                     }
-                    if (kVol && pending >= 0) flush_cell(acc, pending, cs);
+                    if (kVol && pending >= 0) flush_run(pending, cs);
                     if constexpr (kMoments == kStoreMoments) {
                         // the forward image: the same serial sum the forward kernel forms (a
                         // trailing zero sample only turns -0 into +0), scaled by length*step
@@ -1030,7 +1123,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                 double total = 0.0;
 #pragma unroll
                 for (int w = 0; w < kVjpBlock / 32; ++w) total += warp_sums[w][threadIdx.x];
-                partials[((int64_t)view_local * a.tiles_per_view + blockIdx.x) * components +
+                partials[((int64_t)view_local * a.tiles_per_view + tile) * components +
                          threadIdx.x] = total;
             }
         }
@@ -1042,7 +1135,7 @@ template <int kArith, class Field, typename Seed>
 cudaError_t vjp_with(const RayArgs& a, const Field& f, const Seed* cot, int flags, float* acc,
                      double* partials, cudaStream_t stream)
 {
-    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const dim3 grid(ray_blocks(a));
     const bool volume = (flags & DPT_VJP_VOLUME) != 0;
     const bool pose = (flags & (DPT_VJP_POSE12 | DPT_VJP_POSE6 | DPT_VJP_PER_RAY6)) != 0;
     const int mode = (flags & DPT_VJP_POSE12) ? 12 : ((flags & DPT_VJP_PER_RAY6) ? -6 : 6);
@@ -1107,7 +1200,7 @@ cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packe
 cudaError_t launch_forward_moments(const dpt_problem& p, const RayArgs& a, const void* packed,
                                    float* image, float* moments, int64_t stride, cudaStream_t stream)
 {
-    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const dim3 grid(ray_blocks(a));
     const MomentArgs ma{moments, stride, image};
     auto run = [&](auto arith, const auto& f) {
         using FieldT = std::decay_t<decltype(f)>;
@@ -1135,7 +1228,7 @@ cudaError_t launch_pose_from_moments(const dpt_problem& p, const RayArgs& a, con
                                      int64_t stride, const void* cotangent, int flags,
                                      double* partials, cudaStream_t stream)
 {
-    const dim3 grid((unsigned)a.tiles_per_view, (unsigned)a.views);
+    const dim3 grid(ray_blocks(a));
     const int mode = (flags & DPT_VJP_POSE12) ? 12 : ((flags & DPT_VJP_PER_RAY6) ? -6 : 6);
     const MomentArgs ma{const_cast<float*>(moments), stride, nullptr};
     const PlainF32 none{nullptr, p.nx, p.ny, p.nz};
