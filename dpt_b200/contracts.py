@@ -10,7 +10,7 @@ domain raises ``TrialDomainError``.
 from __future__ import annotations
 
 import math
-import struct
+from array import array
 from numbers import Real
 from typing import Any
 
@@ -27,34 +27,41 @@ class TrialDomainError(NumericalError):
     """A prediction or input lies outside its declared domain (status bit 8)."""
 
 
+def _plain_real(value: Any) -> bool:
+    return isinstance(value, Real) and not isinstance(value, bool)
+
+
 def integer(value: Any, name: str, *, minimum: int = 0, maximum: int = 2**31 - 1) -> int:
-    """Require a Python ``int`` (not ``bool``) inside ``[minimum, maximum]``."""
-    if type(value) is not int or not minimum <= value <= maximum:
+    """A Python ``int`` (``bool`` and other subclasses excluded) in ``[minimum, maximum]``."""
+    if type(value) is not int or value < minimum or value > maximum:
         raise ContractError(f"{name} must be an integer in [{minimum}, {maximum}]")
     return value
 
 
 def finite_scalar(value: Any, name: str, *, minimum: float | None = None) -> float:
-    """Accept a finite real scalar with an optional inclusive lower bound."""
-    if isinstance(value, bool) or not isinstance(value, Real):
+    """A real scalar (``bool`` excluded) as a finite Python float, at least ``minimum``."""
+    if not _plain_real(value):
         raise ContractError(f"{name} must be a real scalar")
-    result = float(value)
-    if not math.isfinite(result) or (minimum is not None and result < minimum):
-        qualifier = "finite" if minimum is None else f"finite and at least {minimum}"
-        raise ContractError(f"{name} must be {qualifier}")
-    return result
+    number = float(value)
+    if minimum is None:
+        if not math.isfinite(number):
+            raise ContractError(f"{name} must be finite")
+    elif not (math.isfinite(number) and number >= minimum):
+        raise ContractError(f"{name} must be finite and at least {minimum}")
+    return number
+
+
+# Finite doubles at or above this magnitude round to infinity in binary32 (round to nearest:
+# halfway between the largest binary32 value and 2^128).
+_BINARY32_OVERFLOW = 2.0**128 - 2.0**103
 
 
 def binary32_scalar(value: Any, name: str, *, minimum: float | None = None) -> float:
-    """A finite real scalar rounded once to binary32; overflow to infinity is rejected."""
-    result = finite_scalar(value, name, minimum=minimum)
-    try:
-        result = struct.unpack("f", struct.pack("f", result))[0]
-    except (OverflowError, struct.error) as error:
-        raise ContractError(f"{name} cannot be represented in binary32") from error
-    if not math.isfinite(result):
+    """A finite real scalar rounded once to binary32; a value that rounds to infinity is rejected."""
+    number = finite_scalar(value, name, minimum=minimum)
+    if abs(number) >= _BINARY32_OVERFLOW:
         raise ContractError(f"{name} cannot be represented in binary32")
-    return result
+    return float(array("f", (number,))[0])
 
 
 def finite_tuple(
@@ -65,15 +72,16 @@ def finite_tuple(
     minimum: float | None = 0.0,
     length: int | None = None,
 ) -> tuple[float, ...]:
-    """Validate a non-empty tuple of finite scalars (non-negative unless minimum=None)."""
-    if not isinstance(values, tuple) or not values:
+    """A non-empty tuple of finite scalars (each at least ``minimum`` unless it is None), of
+    ``length`` entries when given, all strictly positive when ``positive``."""
+    if not (isinstance(values, tuple) and len(values) > 0):
         raise ContractError(f"{name} must be a non-empty immutable tuple")
     if length is not None and len(values) != length:
         raise ContractError(f"{name} must contain {length} values")
-    result = tuple(finite_scalar(value, name, minimum=minimum) for value in values)
-    if positive and any(value <= 0.0 for value in result):
+    numbers = [finite_scalar(entry, name, minimum=minimum) for entry in values]
+    if positive and min(numbers) <= 0.0:
         raise ContractError(f"{name} must be positive")
-    return result
+    return tuple(numbers)
 
 
 # Bit -> exception type, in precedence order (input errors first).

@@ -55,14 +55,8 @@ RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status, 
     return a;
 }
 
-}  // namespace dpt
-
-namespace {
-
+// Argument checks shared by every entry point that takes a problem and rays.
 constexpr int64_t kMaxIndex = 2147483647;  // signed 32-bit indexing, as the reference
-constexpr int kMaxViewsPerLaunch = 65535;   // views per launch of the ray kernels
-
-bool aligned(const void* p, uintptr_t bytes) { return (reinterpret_cast<uintptr_t>(p) % bytes) == 0; }
 
 int check_problem(const dpt_problem* p)
 {
@@ -104,6 +98,17 @@ int check_rays(const dpt_problem* p, const dpt_rays* r)
     if (p->ray_kind == DPT_RAYS_BUNDLE && (!r->ray_sources || !r->ray_endpoints)) return DPT_E_NULL;
     return DPT_OK;
 }
+
+}  // namespace dpt
+
+namespace {
+
+using dpt::check_problem;
+using dpt::check_rays;
+
+constexpr int kMaxViewsPerLaunch = 65535;   // views per launch of the ray kernels
+
+bool aligned(const void* p, uintptr_t bytes) { return (reinterpret_cast<uintptr_t>(p) % bytes) == 0; }
 
 int to_code(cudaError_t e) { return e == cudaSuccess ? DPT_OK : (int)e; }
 

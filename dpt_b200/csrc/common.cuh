@@ -111,7 +111,7 @@ __device__ __forceinline__ bool rigid_pose(const double* p)
 // volume accumulator records they touch are shared in L2 instead of each view streaming the
 // whole volume through it (a launch's blocks are dispatched roughly in index order).
 #ifndef DPT_VIEW_GROUP
-#define DPT_VIEW_GROUP 8
+#define DPT_VIEW_GROUP 32
 #endif
 
 // Blocks of a launch over a.views views and a.tiles_per_view tiles per view.

@@ -8,6 +8,10 @@
 
 namespace dpt {
 
+// DPT_OK, or the DPT_E_* code of the first rule a problem (or its ray description) breaks.
+int check_problem(const dpt_problem* p);
+int check_rays(const dpt_problem* p, const dpt_rays* r);
+
 // Fill a RayArgs record for views [view_begin, view_begin + view_count) and blocks of
 // `threads` threads (kBlock for the forward and count kernels, kVjpBlock for the VJP).
 RayArgs make_ray_args(const dpt_problem& p, const dpt_rays& r, int32_t* status, int threads);

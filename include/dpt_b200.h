@@ -259,9 +259,12 @@ int dpt_b200_counts(const dpt_problem* problem, const dpt_rays* rays, double* lo
  * host application owns the GPU memory).  No counterpart in the reference.  The per-block
  * partials live in a fixed 1 MiB device array inside the library (view_count x blocks per
  * view x components <= 131072, else DPT_E_CAPACITY); the FP32 field is read directly.
- * The first call on a device looks up that array's address (call it once before any stream
- * capture); calls that overlap on the GPU share the array and race.  `pose_gradient` is
- * view_count x components (12 packed or 6 local-right); status as dpt_b200_vjp. */
+ * Every call looks up that array's device address on the current device; the first call on
+ * a device also loads the library's device code there, so make it before any stream
+ * capture.  Calls that overlap on the GPU share the array and race.  Arithmetic: FP32,
+ * FP64, compensated or cell-Gauss (the direct-gather form of each); the problem and rays
+ * are checked as by dpt_b200_vjp.  `pose_gradient` is view_count x components (12 packed
+ * or 6 local-right); status as dpt_b200_vjp. */
 int dpt_b200_pose_vjp_fixed(const dpt_problem* problem, const dpt_rays* rays, const float* field,
                             const void* cotangent, int32_t components, double* pose_gradient,
                             int32_t* status, void* stream);

@@ -4,8 +4,8 @@ That entry point serves callers that cannot call cudaMalloc while they run: trac
 guidance loops that reserve their device memory at start-up and hosts that own all GPU
 memory.  Its per-block partials live in a fixed device array inside the library, so two
 calls in a row must both reproduce the pose gradient of dpt_b200_vjp + dpt_b200_finish_pose
-(with caller scratch); this file is collected last so a failure here comes after every
-other test has run.
+(with caller scratch, the same direct-gather sampling); this file is collected last so a
+failure here comes after every other test has run.
 """
 
 from __future__ import annotations
@@ -21,13 +21,23 @@ from scenes import cone_scene, poses_for
 
 pytestmark = pytest.mark.gpu
 
+CASES = [
+    ("float32", "midpoint", 12),
+    ("float32", "midpoint", 6),
+    ("float64", "midpoint", 12),
+    ("compensated", "midpoint", 12),
+    ("float64", "cell_gauss", 6),
+]
 
-@pytest.mark.parametrize("sampling, components", [("float32", 12), ("float32", 6), ("float64", 12)])
-def test_fixed_scratch_pose_vjp_matches_the_allocating_entry_point(sampling, components):
+
+@pytest.mark.parametrize("sampling, integration, components", CASES)
+def test_fixed_scratch_pose_vjp_matches_the_allocating_entry_point(sampling, integration, components):
     grid, geometry, values = cone_scene(views=3, detector=(40, 36))
     poses = torch.tensor(poses_for(3, seed=12), dtype=torch.float64, device="cuda:0")
     precision = "float64" if sampling == "float64" else "float32"
-    spec = ProjectionSpec(57, precision=precision, sampling_precision=sampling)
+    # the allocating path with the same direct gathers the fixed entry point uses
+    spec = ProjectionSpec(57, precision=precision, sampling_precision=sampling, integration=integration,
+                          layout="direct")
     workspace = ProjectionWorkspace(plan_rays(grid, geometry), spec, "cuda:0")
     field = torch.tensor(values, device="cuda:0")
     dtype = torch.float64 if precision == "float64" else torch.float32
@@ -51,13 +61,26 @@ def test_fixed_scratch_pose_vjp_matches_the_allocating_entry_point(sampling, com
 
 
 def test_fixed_scratch_rejects_work_beyond_its_capacity():
-    grid, geometry, values = cone_scene(views=3, detector=(40, 36))
-    spec = ProjectionSpec(9, sampling_precision="float32")
-    workspace = ProjectionWorkspace(plan_rays(grid, geometry), spec, "cuda:0")
+    """A 4096 x 4096 single view needs 65536 blocks x 12 partials, more than the array holds:
+    the call returns DPT_E_CAPACITY before any launch.  Every pointer is a real device buffer
+    of the size the call would use, so a regression returns a wrong code or writes values
+    here, never an out-of-range address."""
+    grid, geometry, values = cone_scene(views=1, detector=(40, 36))
+    workspace = ProjectionWorkspace(plan_rays(grid, geometry), ProjectionSpec(9, sampling_precision="float32"),
+                                    "cuda:0")
     big = N.Problem.from_buffer_copy(workspace.problem)
-    big.rows = big.cols = 4096  # 65536 blocks per view x 12 components > 131072 doubles
-    rays = N.Rays()
-    rays.poses = rays.view_table = 256
-    rays.view_count = 1
-    code = N.library().dpt_b200_pose_vjp_fixed(big, rays, 256, 256, 12, 256, 256, None)
+    big.rows = big.cols = 4096
+    device = "cuda:0"
+    field = torch.tensor(values, device=device)
+    cotangent = torch.zeros(4096 * 4096, dtype=torch.float32, device=device)
+    poses = torch.tensor(poses_for(1, seed=3), dtype=torch.float64, device=device)
+    out = torch.full((1, 12), float("nan"), dtype=torch.float64, device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    rays = workspace.rays(poses)
+    code = N.library().dpt_b200_pose_vjp_fixed(big, rays, field.data_ptr(), cotangent.data_ptr(), 12,
+                                               out.data_ptr(), status.data_ptr(),
+                                               torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
     assert code == -7 and N.library().dpt_b200_error_string(code) == b"a fixed-capacity buffer is too small"
+    assert int(status.item()) == 0
+    assert bool(torch.isnan(out).all())
