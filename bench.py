@@ -61,6 +61,8 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--impl", choices=("dpt_b200", "reference"), default="dpt_b200")
     parser.add_argument("--views", type=int, default=360, help="views per rank")
     parser.add_argument("--size", type=int, default=256, help="grid samples per axis")
+    parser.add_argument("--spacing", type=float, default=None,
+                        help="voxel size in mm (default 0.8 * 256 / size: the full scan's 204.8 mm cube)")
     parser.add_argument("--detector", type=int, default=512)
     parser.add_argument("--samples", type=int, default=1024)
     parser.add_argument("--storage", choices=("float32", "bfloat16", "float16"), default="float32")
@@ -139,7 +141,7 @@ def build_workload(args, device):
     from dpt_b200.geometry import ConeBeamIntrinsics
     from dpt_b200.phantoms import centred_grid, chest_phantom
 
-    spacing = 0.8 * 256.0 / args.size
+    spacing = args.spacing if args.spacing else 0.8 * 256.0 / args.size
     grid = centred_grid((args.size,) * 3, (spacing,) * 3)
     intrinsics = ConeBeamIntrinsics(1000.0, 1500.0, (args.detector, args.detector),
                                     (0.8 * 512.0 / args.detector,) * 2)
@@ -499,8 +501,8 @@ def run_gpu(args) -> None:
         "peak_source": "measured in this run: dpt_b200_read_probe, float4 .cg loads of a 64 MiB L2-resident "
                        "buffer, best of 10 launches of 20 passes",
         "bytes_per_sample": algorithmic_bytes(dominant, storage_bytes),
-        "limiter": "instruction issue (ncu: issue slots 61-70% busy, 'not selected' the top stall; "
-                   "L1 hit 92%, DRAM 1.5 B per realised sample)",
+        "limiter": "FP32 pipe (ncu on the forward with pose moments: FMA pipe 65.6% of active cycles, "
+                   "math-pipe throttle the top stall; L1 hit 92.7%, L2 hit 86.8%, DRAM 0.21 B per realised sample)",
         "hbm": {"peak": hbm_peak, "peak_source": f"{hbm_kind} MEASURED_PEAKS hbm_gbs",
                 "dram_gbs": None if traffic is None else round(traffic / (mean_ms * 1e-3) / 1e9, 1),
                 "frac": None if traffic is None else round(traffic / (mean_ms * 1e-3) / 1e9 / hbm_peak, 4)},
@@ -577,8 +579,10 @@ def run_gpu(args) -> None:
             "vs_baseline": None,
             "dtype": "f32" if args.storage == "float32" else f"f32 ({args.storage} storage)",
             "data": "synthetic (seeded chest-like HU phantom, 60 keV water model; no scanned volume)",
-            "config": {"workload": WORKLOAD if (args.size, args.views, args.detector, args.samples) == (256, 360, 512, 1024)
-                       else f"{args.size}^3, {args.views} views, {args.detector}^2, S={args.samples}",
+            "config": {"workload": WORKLOAD if (args.size, args.views, args.detector, args.samples, args.spacing)
+                       == (256, 360, 512, 1024, None)
+                       else f"{args.size}^3 at {grid.spacing_mm[0]:g} mm, {args.views} views, {args.detector}^2, "
+                            f"S={args.samples}",
                        "grid": [args.size] * 3, "views_per_gpu": len(geometry.views),
                        "detector": [args.detector, args.detector], "samples_per_ray": args.samples,
                        "storage": args.storage, "precision": "fp32",
@@ -1171,7 +1175,7 @@ def run_panels(args) -> None:
     from dpt_b200.plan import plan_rays
 
     device = torch.device("cuda:0")
-    spacing = 0.8 * 256.0 / args.size
+    spacing = args.spacing if args.spacing else 0.8 * 256.0 / args.size
     grid = centred_grid((args.size,) * 3, (spacing,) * 3)
     intrinsics = ConeBeamIntrinsics(1000.0, 1500.0, (args.detector, args.detector),
                                     (0.8 * 512.0 / args.detector,) * 2)
