@@ -74,6 +74,8 @@ def parse() -> argparse.Namespace:
                         help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
     parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
     parser.add_argument("--slots", type=int, default=4, help="serving mode: concurrent request streams")
+    parser.add_argument("--no-autotune", action="store_true", help="serving mode: default detector tiles")
+    parser.add_argument("--no-graphs", action="store_true", help="serving mode: no CUDA graph replay")
     return parser.parse_args()
 
 
@@ -894,7 +896,8 @@ def run_serving(args) -> None:
     sequential_s = time.perf_counter() - start
     del modules
 
-    with ProjectionServer(str(device), slots=args.slots) as server:
+    with ProjectionServer(str(device), slots=args.slots, autotune=not args.no_autotune,
+                          graphs=not args.no_graphs) as server:
         for name, (grid, values) in volumes.items():
             for storage in ("float32", "bfloat16"):
                 server.add_volume(f"{name}:{storage}", grid, values, storage=storage)
@@ -906,6 +909,15 @@ def run_serving(args) -> None:
             server.run_alone(request)
         torch.cuda.synchronize()
         alone_s = time.perf_counter() - start
+        # the same launch sequences back to back on one stream, one synchronisation at the end:
+        # the time the GPU needs for this work with no gap between requests, so
+        # alone_s / chained_s bounds what any overlap of requests can gain
+        chained_s = math.inf
+        for _ in range(2):
+            start = time.perf_counter()
+            server.run_chained(requests)
+            torch.cuda.synchronize()
+            chained_s = min(chained_s, time.perf_counter() - start)
         for _ in range(2):  # warm the served path: workspaces, tiles and graphs on the slots
             saturated(server)
         served_s = min(saturated(server) for _ in range(3))
@@ -931,6 +943,8 @@ def run_serving(args) -> None:
         "speedup_vs_sequential": sequential_s / served_s,
         "sequential_same_arithmetic_requests_per_s": len(requests) / alone_s,
         "speedup_vs_sequential_same_arithmetic": alone_s / served_s,
+        "chained_same_arithmetic_requests_per_s": len(requests) / chained_s,
+        "overlap_bound": alone_s / chained_s,
         "p50_ms": percentile(latencies, 50),
         "p99_ms": percentile(latencies, 99),
         "latency_load_requests_per_s": rate,
@@ -945,9 +959,12 @@ def run_serving(args) -> None:
                    "sequential_same_arithmetic": "the server's own launch sequence per request, one "
                                                  "after another on one stream (BF16 volumes in the "
                                                  "compensated form)",
+                   "chained_same_arithmetic": "the same launch sequences back to back on one stream with "
+                                              "one synchronisation at the end (no gap between requests)",
                    "capacity": "all requests submitted at once, best of 3 after 2 warm rounds",
                    "latency": "Poisson arrivals at 70% of served capacity, 4 rounds",
-                   "slots": args.slots, "memory_budget_gib": 120},
+                   "slots": args.slots, "memory_budget_gib": 120, "autotune": not args.no_autotune,
+                   "graphs": not args.no_graphs},
     }
     print(json.dumps(line), flush=True)
 

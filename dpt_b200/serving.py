@@ -10,7 +10,10 @@ adds on top of the projector:
   memory fits the budget (first fit over a bounded look-ahead, so a large request
   waiting for memory does not block small ones behind it);
 * every admitted request runs on its own CUDA stream, so requests that arrive while
-  others are on the GPU overlap on the device;
+  others are on the GPU overlap on the device; requests that fill the GPU on their own
+  (``exclusive_samples`` nominal ray-samples and more) run one at a time, with smaller ones
+  beside them, because two large requests interleave their blocks and evict each other's
+  field copy and accumulator records from L2;
 * repeated request shapes below ``graph_samples`` nominal ray-samples replay a captured
   CUDA graph of their launch sequence (larger requests are launch-count bound no more, and
   a replay must copy its outputs out of the graph's static buffers);
@@ -103,12 +106,14 @@ class Admission:
             raise ContractError(f"request needs {nbytes} bytes, more than the {self.budget}-byte budget")
         self.waiting.append((item, int(nbytes)))
 
-    def take(self, free_slots: int) -> list[tuple[Any, int]]:
+    def take(self, free_slots: int, eligible: Callable[[Any], bool] | None = None) -> list[tuple[Any, int]]:
+        """Start what fits, in arrival order; ``eligible(item)`` (called in that order, once
+        per candidate that fits the budget) may hold an item back for now."""
         started: list[tuple[Any, int]] = []
         index = 0
         while free_slots > 0 and index < min(len(self.waiting), self.lookahead):
             item, nbytes = self.waiting[index]
-            if self.in_use + nbytes <= self.budget:
+            if self.in_use + nbytes <= self.budget and (eligible is None or eligible(item)):
                 del self.waiting[index]
                 self.in_use += nbytes
                 self.peak = max(self.peak, self.in_use)
@@ -180,6 +185,8 @@ class _Job:
     outputs: dict = field(default_factory=dict)
     workspace: Any = None
     key: Any = None  # request class: volume, geometry, samples, precision, kind
+    large: bool = False  # fills the GPU on its own: runs while no other large request does
+    private_host: bool = False  # own pinned readback buffers instead of the slot's
 
 
 class _Slot:
@@ -219,7 +226,7 @@ class ProjectionServer:
 
     def __init__(self, device: str = "cuda:0", *, memory_budget_bytes: int = 120 << 30, slots: int = 4,
                  graphs: bool = True, autotune: bool = True, workspaces_per_slot: int = 64,
-                 graph_samples: int = 1 << 30) -> None:
+                 graph_samples: int = 1 << 30, exclusive_samples: int = 1 << 30) -> None:
         import torch
 
         self.torch = torch
@@ -232,6 +239,8 @@ class ProjectionServer:
         self.tuner = TileTuner()
         self.graphs = graphs
         self.graph_samples = graph_samples
+        self.exclusive_samples = exclusive_samples
+        self.large_running = 0
         self.autotune = autotune
         self.workspaces_per_slot = workspaces_per_slot
         self.volumes: dict[str, _Volume] = {}
@@ -279,6 +288,7 @@ class ProjectionServer:
         future: Future = Future()
         job = _Job(request, future, time.perf_counter())
         job.nbytes = self.request_bytes(request)
+        job.large = self._large(request)
         job.key = (request.volume, batched(request.geometry), request.samples_per_ray, request.precision,
                    request.kind)
         with self.lock:
@@ -300,6 +310,24 @@ class ProjectionServer:
         job.event.synchronize()
         return self._finish(job)
 
+    def run_chained(self, requests: list[ProjectionRequest]) -> list[ProjectionResult]:
+        """Enqueue the launch sequences of ``requests`` back to back on the caller's stream with
+        no synchronisation between them (the same arithmetic as ``run_alone``); return their
+        results once the stream has finished them all."""
+        if self._alone is None:
+            self._alone = _Slot(self.torch, self.device, -1, self.torch.cuda.current_stream(self.device))
+        jobs = []
+        for request in requests:
+            job = _Job(request, Future(), time.perf_counter())
+            job.slot = self._alone
+            job.private_host = True
+            job.started = time.perf_counter()
+            self._launch(job, use_graph=False)
+            jobs.append(job)
+        if jobs:
+            jobs[-1].event.synchronize()
+        return [self._finish(job) for job in jobs]
+
     def close(self) -> None:
         with self.lock:
             self.closed = True
@@ -314,6 +342,15 @@ class ProjectionServer:
         self.close()
 
     # ---------------------------------------------------------- sizing
+    def _large(self, request: ProjectionRequest) -> bool:
+        """Whether a request fills the GPU on its own (nominal ray-samples of its passes): such
+        requests run one at a time, because two of them interleave their blocks and evict each
+        other's field copy and accumulator records from L2."""
+        from .plan import batched
+
+        passes = 1 if request.kind == "forward" else 2
+        return batched(request.geometry).pixels * request.samples_per_ray * passes >= self.exclusive_samples
+
     def _small(self, request: ProjectionRequest) -> bool:
         """Whether a request is small enough for graph replay to pay (nominal ray-samples)."""
         from .plan import batched
@@ -346,7 +383,19 @@ class ProjectionServer:
                 if self.closed and not self.admission.waiting:
                     return
                 free = [slot for slot in self.slots if not slot.busy]
-                taken = self.admission.take(len(free))
+                large_now = self.large_running
+
+                def eligible(job: _Job) -> bool:
+                    nonlocal large_now
+                    if not job.large:
+                        return True
+                    if large_now:
+                        return False
+                    large_now += 1
+                    return True
+
+                taken = self.admission.take(len(free), eligible)
+                self.large_running = large_now
                 for job, _ in taken:
                     # prefer a free slot that already holds this class's workspace and graph
                     slot = next((s for s in free if job.key in s.classes), free[0])
@@ -366,9 +415,9 @@ class ProjectionServer:
                     self.lock.notify_all()
 
     def _startable(self) -> bool:
-        if not self.admission.waiting:
+        if not self.admission.waiting or all(slot.busy for slot in self.slots):
             return False
-        return any(not slot.busy for slot in self.slots)
+        return not self.large_running or any(not job.large for job, _ in self.admission.waiting)
 
     def _complete(self) -> None:
         while True:
@@ -393,6 +442,8 @@ class ProjectionServer:
                 job.future.set_exception(error)
             with self.lock:
                 job.slot.busy = False
+                if job.large:
+                    self.large_running -= 1
                 self.admission.release(job.nbytes)
                 self.lock.notify_all()
 
@@ -488,7 +539,9 @@ class ProjectionServer:
         with torch.cuda.stream(slot.stream):
             state = slot.graphs.get(key) if use_graph else None
             if state is None:
-                inputs = {"poses": self._poses(request, views, slot), "target": self._target(request, ws)}
+                # chained requests stage no host data through the slot's shared pinned buffer
+                staging = None if job.private_host else slot
+                inputs = {"poses": self._poses(request, views, staging), "target": self._target(request, ws)}
                 outputs = self._body(ws, volume.field, inputs, request)
                 if use_graph:
                     self._capture(slot, key, ws, volume.field, request, inputs)
@@ -499,12 +552,19 @@ class ProjectionServer:
                     inputs["target"].copy_(self._target(request, ws), non_blocking=True)
                 graph.replay()
                 outputs = {name: value.clone() for name, value in outputs.items()}
-            status_host = slot.pinned("status", views, torch.int32)
+            # a slot runs one request at a time and reuses its pinned buffers; requests chained
+            # without synchronisation each need their own
+            def host(name: str, count: int, dtype):
+                if job.private_host:
+                    return torch.empty(count, dtype=dtype, pin_memory=True)
+                return slot.pinned(name, count, dtype)
+
+            status_host = host("status", views, torch.int32)
             status_host.copy_(ws.status, non_blocking=True)
             ws.status.zero_()
             job.outputs = dict(outputs, status=status_host)
             if "loss" in outputs:  # read back with the status, no host synchronisation later
-                loss_host = slot.pinned("loss", 1, torch.float64)
+                loss_host = host("loss", 1, torch.float64)
                 loss_host.copy_(outputs["loss"].reshape(1), non_blocking=True)
                 job.outputs["loss_host"] = loss_host
             job.workspace = ws

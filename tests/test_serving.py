@@ -122,6 +122,30 @@ def test_results_are_the_same_alone_and_in_the_mix(graphs):
 
 
 @pytest.mark.gpu
+def test_chained_requests_match_the_same_requests_alone():
+    """run_chained (the launch sequences back to back, one synchronisation) returns what
+    run_alone returns for each request: its own readback buffers, no shared staging."""
+    from dpt_b200.serving import ProjectionServer
+
+    scenes, requests = _requests(seed=5, count=10)
+    with ProjectionServer("cuda:0", slots=1, graphs=False, autotune=False) as server:
+        for name, (grid, values) in scenes.items():
+            server.add_volume(name, grid, values)
+        alone = [server.run_alone(request) for request in requests]
+        chained = server.run_chained(requests)
+    for request, a, c in zip(requests, alone, chained, strict=True):
+        np.testing.assert_array_equal(c.image.cpu().numpy(), a.image.cpu().numpy())
+        if request.kind == "volume":
+            va, vc = a.volume_gradient.cpu().numpy(), c.volume_gradient.cpu().numpy()
+            assert np.linalg.norm(va - vc) <= 1e-6 * np.linalg.norm(va)
+        if request.kind == "pose":
+            np.testing.assert_allclose(c.pose_gradient.cpu().numpy(), a.pose_gradient.cpu().numpy(),
+                                       rtol=1e-10, atol=1e-13)
+        if request.kind != "forward":
+            assert c.loss == pytest.approx(a.loss, rel=1e-12)
+
+
+@pytest.mark.gpu
 def test_budget_limits_concurrency():
     from dpt_b200.serving import ProjectionServer
 
@@ -172,3 +196,22 @@ def test_shared_field_copies_and_scratch_pool_match_private_workspaces():
                 g_got, _ = s.vjp(field, poses_v, cot, volume=True, pose=None)
                 assert torch.linalg.norm(g_got - g_expected) <= 1e-6 * torch.linalg.norm(g_expected)
         assert copies.bytes() > 0
+
+
+def test_admission_holds_back_ineligible_items_without_blocking_the_rest():
+    admission = Admission(1000, lookahead=8)
+    for name in ("big1", "small1", "big2", "small2"):
+        admission.offer(name, 10)
+    # one large item may start: the second waits, the small ones pass it
+    started = [0]
+
+    def eligible(name):
+        if name.startswith("big"):
+            if started[0]:
+                return False
+            started[0] += 1
+        return True
+
+    assert [name for name, _ in admission.take(4, eligible)] == ["big1", "small1", "small2"]
+    assert [name for name, _ in admission.waiting] == ["big2"]
+    assert [name for name, _ in admission.take(4)] == ["big2"]
