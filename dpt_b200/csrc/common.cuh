@@ -673,9 +673,25 @@ struct CellRun {
 // axis meets next is kept as an exact float coordinate; it is crossed at sample coordinate
 // (plane - entry) / sv, computed as (plane - entry) * (1 / sv), or never (+inf) when it lies
 // outside the cell planes 0..n-1 or the ray does not move on that axis.
+// Power sums of short runs, tabulated once per block: entry n holds (n, S1, S2, S3) for
+// j = 0..n-1 as walk_cells forms them (exact integers rounded once to FP32, S3 = S1 * S1 in
+// FP32), so a run of at most kRunSumTable samples reads its sums instead of forming them.
+constexpr int kRunSumTable = 64;
+__device__ __forceinline__ float4 run_power_sums(int n)
+{
+    const unsigned m = (unsigned)n;
+    const unsigned s1 = m * (m - 1u) / 2u;
+    const float f1 = (float)s1;
+    return make_float4((float)n, f1, (float)(s1 * (2u * m - 1u) / 3u), f1 * f1);
+}
+__device__ __forceinline__ void fill_run_sums(float4* table)
+{
+    for (int n = threadIdx.x; n <= kRunSumTable; n += blockDim.x) table[n] = run_power_sums(n);
+}
+
 template <typename Action>
 __device__ __forceinline__ void walk_cells(const FieldDims& dims, const float* entry, const float* sv,
-                                           int first, int last, Action action)
+                                           int first, int last, Action action, const float4* sums = nullptr)
 {
     const int shape[3] = {dims.nx, dims.ny, dims.nz};
     const float top_plane[3] = {dims.mx, dims.my, dims.mz};  // n - 1
@@ -730,18 +746,25 @@ __device__ __forceinline__ void walk_cells(const FieldDims& dims, const float* e
             r.cell = (lower[2] * dims.ny + lower[1]) * dims.nx + lower[0];
             // power sums of j = 0..n-1 (exact integers, rounded once to FP32); 32-bit
             // arithmetic is exact up to n = 1024
-            if (r.n <= 1024) {
-                const unsigned m = (unsigned)r.n;
-                const unsigned s1 = m * (m - 1u) / 2u;
-                r.s1 = (float)s1;
-                r.s2 = (float)(s1 * (2u * m - 1u) / 3u);
+            if (sums && r.n <= kRunSumTable) {
+                const float4 e = sums[r.n];
+                r.nf = e.x;
+                r.s1 = e.y;
+                r.s2 = e.z;
+                r.s3 = e.w;
             } else {
-                const int64_t m = r.n;
-                r.s1 = (float)(m * (m - 1) / 2);
-                r.s2 = (float)(m * (m - 1) * (2 * m - 1) / 6);
+                if (r.n <= 1024) {
+                    const float4 e = run_power_sums(r.n);
+                    r.s1 = e.y;
+                    r.s2 = e.z;
+                } else {
+                    const int64_t m = r.n;
+                    r.s1 = (float)(m * (m - 1) / 2);
+                    r.s2 = (float)(m * (m - 1) * (2 * m - 1) / 6);
+                }
+                r.nf = (float)r.n;
+                r.s3 = r.s1 * r.s1;
             }
-            r.nf = (float)r.n;
-            r.s3 = r.s1 * r.s1;
             action(r);
         }
         i = end;

@@ -65,10 +65,12 @@ template <int kArith, class Field, typename Out>
 __global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, Out* __restrict__ image)
 {
     __shared__ ViewShared vs;
+    __shared__ float4 run_sums[kArith == DPT_ARITH_F32C ? kRunSumTable + 1 : 1];
+    if (kArith == DPT_ARITH_F32C) fill_run_sums(run_sums);
     int view_local, tile;
     block_work(a, &view_local, &tile);
     const int view = a.view_begin + view_local;
-    stage_view(a, view, vs);
+    stage_view(a, view, vs);  // synchronises the block (the table is ready)
     int pixel;
     if (!ray_of_thread(a, tile, &pixel)) return;
 
@@ -387,7 +389,7 @@ __global__ void __launch_bounds__(kForwardBlock) k_forward(RayArgs a, Field f, O
                             PolyCache<Field, false> cell;
                             cell.fetch(f, run.lx, run.ly, run.lz, run.cell);
                             acc.add(run_sum(run, run_poly(cell.c, run.f)));
-                        });
+                        }, run_sums);
                     }
                     total = acc.value();
                 }

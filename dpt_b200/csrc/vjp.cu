@@ -148,6 +148,8 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                   "split pose moments: FP32 or compensated arithmetic, pose only");
     __shared__ ViewShared vs;
     __shared__ double warp_sums[kVjpBlock / 32][12];
+    __shared__ float4 run_sums[kArith == DPT_ARITH_F32C && kMoments != kLoadMoments ? kRunSumTable + 1 : 1];
+    if (kArith == DPT_ARITH_F32C && kMoments != kLoadMoments) fill_run_sums(run_sums);
     // alpha_i = (i + 0.5) / S of the FP32 pose moments, each one IEEE division, tabulated
     // once per block for the first kAlphaTable samples (later samples divide directly)
     __shared__ float alpha_table[kArith == DPT_ARITH_F32 && kPose && kMoments != kLoadMoments ? kAlphaTable : 1];
@@ -947,7 +949,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                                           nf * (fxy * fz))));
                                     scatter_moments(run.cell, m);
                                 }
-                            });
+                            }, run_sums);
                         }
                         words[0] = mean.sum;
                         words[1] = mean.carry;
