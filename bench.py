@@ -530,15 +530,35 @@ def run_gpu(args) -> None:
     h2d = host_field.numel() * host_field.element_size() + host_target.numel() * 4 + host_tangent.numel() * 8
     d2h = out_image.numel() * 4 + out_grad.numel() * out_grad.element_size() + out_pose.numel() * 8 + 8
 
+    # The same step through the public Projector with host buffers.  The target upload runs on a
+    # copy stream beside the forward and the image download beside the VJP; the main stream
+    # waits for both, so every copy is inside the step's events.
+    copies = torch.cuda.Stream(device)
+
     def e2e_step():
-        f = host_field.to(device, non_blocking=True)
-        t = host_target.to(device, non_blocking=True)
-        xi = host_tangent.to(device, non_blocking=True)
-        loss, image, gf, gp = step(f, t, xi)
-        out_loss.copy_(loss, non_blocking=True)
-        out_image.copy_(image, non_blocking=True)
+        main = torch.cuda.current_stream(device)
+        f = host_field.to(device, non_blocking=True).detach().requires_grad_(True)
+        xi = host_tangent.to(device, non_blocking=True).detach().requires_grad_(True)
+        copies.wait_stream(main)
+        with torch.cuda.stream(copies):
+            t = host_target.to(device, non_blocking=True)
+        image = projector(f, xi)
+        forward_done = torch.cuda.Event()
+        forward_done.record(main)
+        main.wait_stream(copies)
+        t.record_stream(main)
+        residual = image - t
+        loss = 0.5 * (residual.double() * residual.double()).sum()
+        with torch.cuda.stream(copies):
+            copies.wait_event(forward_done)
+            image.record_stream(copies)
+            out_image.copy_(image.detach(), non_blocking=True)
+        gf, gp = torch.autograd.grad(loss, (f, xi))
+        reduce_volume_gradient(gf)
+        out_loss.copy_(loss.detach(), non_blocking=True)
         out_grad.copy_(gf, non_blocking=True)
         out_pose.copy_(gp, non_blocking=True)
+        main.wait_stream(copies)
 
     e2e_ms, _, _, _ = timer.run(e2e_step, lambda: ws, args.steps, 1, dist)
 
