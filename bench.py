@@ -76,6 +76,10 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--slots", type=int, default=4, help="serving mode: concurrent request streams")
     parser.add_argument("--no-autotune", action="store_true", help="serving mode: default detector tiles")
     parser.add_argument("--no-graphs", action="store_true", help="serving mode: no CUDA graph replay")
+    parser.add_argument("--no-packing", action="store_true",
+                        help="serving mode: no packed launches of small forward requests")
+    parser.add_argument("--pack-samples", type=int, default=1 << 26,
+                        help="serving mode: forward requests below this many nominal ray-samples may be packed")
     return parser.parse_args()
 
 
@@ -855,6 +859,58 @@ def serving_requests(args, device):
     return volumes, requests
 
 
+def small_burst(args, server, volumes) -> dict:
+    """128 small forward requests submitted at once (64^3 / 128^3 volumes in FP32 or BF16, 1-4
+    views, 128^2 or 256^2 detectors, S 128 or 256: DRR-sized previews), served with packed
+    launches, served without them, and run one after another through the server's launch
+    sequence; requests/s of each (best of 3 after a warm round)."""
+    import numpy as np
+    import torch
+
+    from dpt_b200.geometry import ConeBeamIntrinsics
+    from dpt_b200.serving import ProjectionRequest
+
+    rng = np.random.default_rng(args.seed + 11)
+    requests = []
+    for _ in range(128):
+        name = ("v64", "v128")[int(rng.integers(2))]
+        storage = "bfloat16" if rng.random() < 0.5 else "float32"
+        views = int(rng.integers(1, 5))
+        detector = int(rng.choice((128, 256)))
+        samples = int(rng.choice((128, 256)))
+        pitch = 409.6 / detector
+        geometry = ConeBeamIntrinsics(1000.0, 1500.0, (detector, detector), (pitch, pitch)).batch(
+            tuple(2.0 * math.pi * k / views + float(rng.uniform(0, 0.1)) for k in range(views)))
+        requests.append(ProjectionRequest(f"{name}:{storage}", geometry, samples, "forward"))
+
+    def served() -> float:
+        start = time.perf_counter()
+        results = [future.result() for future in [server.submit(r) for r in requests]]
+        return max(r.finished for r in results) - start
+
+    def alone() -> float:
+        start = time.perf_counter()
+        for request in requests:
+            server.run_alone(request)
+        torch.cuda.synchronize()
+        return time.perf_counter() - start
+
+    out = {}
+    packs = server.packs
+    for name, packing, run in (("served_packed", True, served), ("served_unpacked", False, served),
+                               ("sequential_same_arithmetic", True, alone)):
+        server.packing = packing
+        run()
+        out[name + "_requests_per_s"] = len(requests) / min(run() for _ in range(3))
+    server.packing = True
+    out["packed_launches"] = server.packs - packs
+    out["speedup_packed_vs_sequential_same_arithmetic"] = (out["served_packed_requests_per_s"]
+                                                           / out["sequential_same_arithmetic_requests_per_s"])
+    out["speedup_packed_vs_unpacked"] = out["served_packed_requests_per_s"] / out["served_unpacked_requests_per_s"]
+    out["requests"] = len(requests)
+    return out
+
+
 def run_serving(args) -> None:
     """Served mixed stream against the same requests run one after another through the plain
     FP32 projector (and, for reference, through the server's own launch sequence alone).
@@ -917,7 +973,8 @@ def run_serving(args) -> None:
     del modules
 
     with ProjectionServer(str(device), slots=args.slots, autotune=not args.no_autotune,
-                          graphs=not args.no_graphs) as server:
+                          graphs=not args.no_graphs, packing=not args.no_packing,
+                          pack_samples=args.pack_samples) as server:
         for name, (grid, values) in volumes.items():
             for storage in ("float32", "bfloat16"):
                 server.add_volume(f"{name}:{storage}", grid, values, storage=storage)
@@ -940,7 +997,9 @@ def run_serving(args) -> None:
             chained_s = min(chained_s, time.perf_counter() - start)
         for _ in range(2):  # warm the served path: workspaces, tiles and graphs on the slots
             saturated(server)
+        packs, packed = server.packs, server.packed_requests
         served_s = min(saturated(server) for _ in range(3))
+        packs, packed = (server.packs - packs) / 3, (server.packed_requests - packed) / 3
         rng = np.random.default_rng(args.seed + 7)
         rate = 0.7 * len(requests) / served_s
         latencies = []
@@ -954,6 +1013,7 @@ def run_serving(args) -> None:
                     time.sleep(delay)
                 futures.append(server.submit(request))
             latencies += [future.result().latency * 1e3 for future in futures]
+        burst = small_burst(args, server, volumes) if not args.no_packing else None
     samples_total = sum(sum(v.pixels for v in r.geometry.views) * r.samples_per_ray for r in requests)
     line = {
         "metric": "served mixed projection stream",
@@ -970,6 +1030,9 @@ def run_serving(args) -> None:
         "latency_load_requests_per_s": rate,
         "latency_samples": len(latencies),
         "requests": len(requests),
+        "packed_launches_per_round": packs,
+        "packed_requests_per_round": packed,
+        "small_burst": burst,
         "nominal_ray_samples": samples_total,
         "higher_is_better": True,
         "config": {"workload": "Poisson mix: 64^3/128^3/256^3/512x512x128 volumes FP32|BF16, 1-64 views, "
@@ -984,7 +1047,8 @@ def run_serving(args) -> None:
                    "capacity": "all requests submitted at once, best of 3 after 2 warm rounds",
                    "latency": "Poisson arrivals at 70% of served capacity, 4 rounds",
                    "slots": args.slots, "memory_budget_gib": 120, "autotune": not args.no_autotune,
-                   "graphs": not args.no_graphs},
+                   "graphs": not args.no_graphs, "packing": not args.no_packing,
+                   "pack_samples": args.pack_samples},
     }
     print(json.dumps(line), flush=True)
 

@@ -15,7 +15,8 @@ from pathlib import Path
 from .contracts import ContractError
 
 LIBRARY_PATH = Path(__file__).resolve().parent / "_lib" / "libdpt_b200.so"
-ABI_VERSION = 3
+ABI_VERSION = 4
+MAX_PACK = 64  # DPT_MAX_PACK: problems of one packed forward launch
 
 # Mirrors of the header's enums.
 F32, F64, F16, BF16 = 0, 1, 2, 3
@@ -39,6 +40,7 @@ EXPORTS = (
     "dpt_b200_pose_partials_bytes",
     "dpt_b200_prepare_field",
     "dpt_b200_forward",
+    "dpt_b200_forward_packed",
     "dpt_b200_vjp",
     "dpt_b200_finish_pose",
     "dpt_b200_fold_volume",
@@ -117,6 +119,7 @@ _SIGNATURES = {
     "dpt_b200_pose_partials_bytes": ([_P, _I], ctypes.c_size_t),
     "dpt_b200_prepare_field": ([_P, _V, _V, _V, _V, _V], ctypes.c_int),
     "dpt_b200_forward": ([_P, _R, _V, _V, _V, _V], ctypes.c_int),
+    "dpt_b200_forward_packed": ([_I, _P, _R, _V, _V, _V, _V], ctypes.c_int),
     "dpt_b200_vjp": ([_P, _R, _V, _V, _I, _V, _V, _V, _V], ctypes.c_int),
     "dpt_b200_finish_pose": ([_P, _I, _I, _I, _V, _V, _I, _V, _V], ctypes.c_int),
     "dpt_b200_fold_volume": ([_P, _V, _V, _I, _V, _I, _I, _V, _V], ctypes.c_int),

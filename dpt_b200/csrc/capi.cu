@@ -204,6 +204,30 @@ int dpt_b200_forward(const dpt_problem* p, const dpt_rays* r, const void* packed
     });
 }
 
+int dpt_b200_forward_packed(int32_t count, const dpt_problem* problems, const dpt_rays* rays,
+                            const void* const* packed, void* const* images, int32_t* const* status, void* stream)
+{
+    if (count < 1) return DPT_E_SHAPE;
+    if (count > DPT_MAX_PACK) return DPT_E_CAPACITY;
+    if (!problems || !rays || !packed || !images || !status) return DPT_E_NULL;
+    dpt::RayArgs args[DPT_MAX_PACK];
+    for (int32_t k = 0; k < count; ++k) {
+        const dpt_problem* p = problems + k;
+        int code = check_problem(p);
+        if (code != DPT_OK) return code;
+        if ((code = check_rays(p, rays + k)) != DPT_OK) return code;
+        if (!packed[k] || !images[k] || !status[k]) return DPT_E_NULL;
+        if (!aligned(packed[k], 16)) return DPT_E_ALIGN;
+        // one kernel instantiation serves the pack
+        if (p->arith != problems[0].arith || p->layout != problems[0].layout ||
+            p->image_dtype != problems[0].image_dtype)
+            return DPT_E_FLAGS;
+        if (rays[k].view_count > kMaxViewsPerLaunch) return DPT_E_RANGE;
+        args[k] = dpt::make_ray_args(*p, rays[k], status[k], dpt::kForwardBlock);
+    }
+    return to_code(dpt::launch_forward_packed(count, problems, args, packed, images, static_cast<cudaStream_t>(stream)));
+}
+
 size_t dpt_b200_moments_bytes(const dpt_problem* p, int32_t view_count)
 {
     if (check_problem(p) != DPT_OK || view_count < 1) return 0;

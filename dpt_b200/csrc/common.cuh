@@ -32,6 +32,7 @@ constexpr int kForwardBlock = DPT_FORWARD_THREADS;  // threads per block of the 
 #endif
 constexpr int kVjpBlock = DPT_VJP_THREADS;  // threads per block of the VJP kernel
 constexpr int kDefaultBlockCols = 16;  // default block tile: 16 x 16 detector pixels
+constexpr int kMaxPack = DPT_MAX_PACK;  // problems of one packed forward launch
 
 struct Grid {
     int nx, ny, nz;
@@ -120,10 +121,9 @@ __host__ __device__ __forceinline__ unsigned ray_blocks(const RayArgs& a)
     return (unsigned)a.tiles_per_view * (unsigned)a.views;
 }
 
-// (view within the launch, detector tile) of this block.
-__device__ __forceinline__ void block_work(const RayArgs& a, int* view_local, int* tile)
+// (view within the launch, detector tile) of block b of the launch's order.
+__device__ __forceinline__ void block_work_at(const RayArgs& a, int b, int* view_local, int* tile)
 {
-    const int b = (int)blockIdx.x;
     const int per_group = a.view_group * a.tiles_per_view;
     const int g = b / per_group;
     const int r = b - g * per_group;
@@ -132,6 +132,12 @@ __device__ __forceinline__ void block_work(const RayArgs& a, int* view_local, in
     const int t = r / views;
     *tile = t;
     *view_local = first + (r - t * views);
+}
+
+// (view within the launch, detector tile) of this block.
+__device__ __forceinline__ void block_work(const RayArgs& a, int* view_local, int* tile)
+{
+    block_work_at(a, (int)blockIdx.x, view_local, tile);
 }
 
 // Ray index inside its view -> (pixel) for the tiled panel mapping, or the bundle index.

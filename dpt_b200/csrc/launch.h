@@ -27,6 +27,9 @@ cudaError_t launch_prepare_field(const dpt_problem& p, const void* field, void* 
                                  const double* poses, int32_t* status, cudaStream_t stream);
 cudaError_t launch_forward(const dpt_problem& p, const RayArgs& a, const void* packed, void* image,
                            cudaStream_t stream);
+// One launch over `count` problems that share arith, layout and image dtype.
+cudaError_t launch_forward_packed(int count, const dpt_problem* problems, const RayArgs* args,
+                                  const void* const* packed, void* const* images, cudaStream_t stream);
 cudaError_t launch_counts(const dpt_problem& p, const RayArgs& a, double* lower, double* upper,
                           int32_t* realised, cudaStream_t stream);
 cudaError_t launch_vjp(const dpt_problem& p, const RayArgs& a, const void* packed,

@@ -25,6 +25,8 @@ call starts clean.
 
 from __future__ import annotations
 
+import contextlib
+import ctypes
 import threading
 import weakref
 from dataclasses import dataclass
@@ -618,6 +620,68 @@ class ProjectionWorkspace:
         if flat.stride() != (1,):
             flat = flat.clone()
         return flat
+
+
+def forward_packed(calls, *, checked: bool = True) -> list[torch.Tensor]:
+    """Optical depth of several workspaces in one launch.
+
+    ``calls`` is a sequence of ``(workspace, field, poses)`` or ``(workspace, field, poses,
+    out)``: at most ``N.MAX_PACK`` of them, on one device, with one sampling arithmetic, field
+    layout and image dtype; a workspace may appear more than once, with one field (its
+    sampling copy is shared by those calls) and any poses.  Each field is validated (and its
+    sampling copy written) as by ``ProjectionWorkspace.forward``; one launch then walks the (view, tile) blocks of every call,
+    so many small projections fill the GPU without a launch (and a tail) each.  Every image
+    equals that workspace's own forward bit for bit.  Returns the images in call order."""
+    calls = list(calls)
+    if not 1 <= len(calls) <= N.MAX_PACK:
+        raise ContractError(f"a packed forward takes 1 to {N.MAX_PACK} calls")
+    spaces = [call[0] for call in calls]
+    first = spaces[0]
+    for ws in spaces:
+        if not isinstance(ws, ProjectionWorkspace) or ws.device != first.device:
+            raise ContractError("packed calls need projection workspaces on one device")
+        if (ws.spec.arith, ws.problem.layout, ws.spec.image_code) != (first.spec.arith, first.problem.layout,
+                                                                    first.spec.image_code):
+            raise ContractError("packed calls need one sampling arithmetic, field layout and image dtype")
+    with contextlib.ExitStack() as stack, torch.cuda.device(first.device):
+        for ws in dict.fromkeys(spaces):  # each workspace once, in call order
+            stack.enter_context(ws.lock)
+        count = len(calls)
+        problems = (N.Problem * count)()
+        rays = (N.Rays * count)()
+        copies = (ctypes.c_void_p * count)()
+        images = (ctypes.c_void_p * count)()
+        status = (ctypes.c_void_p * count)()
+        outs, keep, fields_of = [], [], {}
+        for k, call in enumerate(calls):
+            ws, field, poses = call[0], call[1], call[2]
+            out = call[3] if len(call) > 3 else None
+            # a workspace holds one sampling copy: it repeats in a pack only with one field
+            if ws.problem.layout != N.LAYOUT_DIRECT and fields_of.setdefault(id(ws), field) is not field:
+                raise ContractError("a workspace repeats in a packed forward only with the same field")
+            field = ws.check_field(field)
+            poses = ws.check_poses(poses)
+            if out is None:
+                out = torch.empty(ws.plan.image_shape, dtype=ws.spec.image_dtype, device=ws.device)
+            elif (tuple(out.shape) != ws.plan.image_shape or out.dtype != ws.spec.image_dtype
+                  or out.device != ws.device or not out.is_contiguous()):
+                raise ContractError("out must match the projector's shape, dtype and input device")
+            copy = ws.prepare_field(field, poses)
+            ws._moments_for = None
+            problems[k] = ws.problem
+            rays[k] = ws.rays(poses)
+            copies[k] = copy.data_ptr()
+            images[k] = out.data_ptr()
+            status[k] = ws.status.data_ptr()
+            outs.append(out)
+            keep.append((field, poses, copy))
+        N.check(N.library().dpt_b200_forward_packed(count, problems, rays, copies, images, status,
+                                                    _stream(first.device)), "forward_packed")
+        for ws in dict.fromkeys(spaces):
+            ws.launches += 1
+            if checked and ws.spec.validate != "never":
+                ws.consume_status()
+        return outs
 
 
 def prepare_projection(grid: GridSpec, geometry, spec: ProjectionSpec, *,

@@ -17,11 +17,20 @@ adds on top of the projector:
 * repeated request shapes below ``graph_samples`` nominal ray-samples replay a captured
   CUDA graph of their launch sequence (larger requests are launch-count bound no more, and
   a replay must copy its outputs out of the graph's static buffers);
+* forward requests below ``pack_samples`` nominal ray-samples that wait together, on volumes
+  of one storage dtype and at one precision, run as one packed launch on one slot (up to
+  ``MAX_PACK`` of them: one block per (request, view, tile) item of them all), so a burst of
+  small requests costs one launch instead of one launch sequence each;
 * the detector tile of each request class comes from a small autotuner that times the
   candidate tiles once per class and keeps the fastest.
 
 Results are exactly those of the same request run alone: the kernels are the same and
-requests share no scratch (each slot owns its workspaces).
+requests share no scratch (each slot owns its workspaces).  Packed launches take their
+workspaces from one server-wide set (one per request class, kept across packs, so a pack of
+classes its slot has not seen creates nothing) and run one at a time per storage dtype and
+precision; requests of one class
+packed together share that class's workspace and its status words, so a status bit one of
+them raises is reported to each of them.
 """
 
 from __future__ import annotations
@@ -123,6 +132,22 @@ class Admission:
                 index += 1
         return started
 
+    def take_matching(self, match: Callable[[Any], bool], limit: int) -> list[tuple[Any, int]]:
+        """Start up to ``limit`` more waiting items for which ``match(item)`` holds and that fit
+        the budget, in arrival order over the whole queue (companions of a packed launch)."""
+        started: list[tuple[Any, int]] = []
+        index = 0
+        while len(started) < limit and index < len(self.waiting):
+            item, nbytes = self.waiting[index]
+            if self.in_use + nbytes <= self.budget and match(item):
+                del self.waiting[index]
+                self.in_use += nbytes
+                self.peak = max(self.peak, self.in_use)
+                started.append((item, nbytes))
+            else:
+                index += 1
+        return started
+
     def release(self, nbytes: int) -> None:
         self.in_use -= int(nbytes)
         if self.in_use < 0:
@@ -187,6 +212,8 @@ class _Job:
     key: Any = None  # request class: volume, geometry, samples, precision, kind
     large: bool = False  # fills the GPU on its own: runs while no other large request does
     private_host: bool = False  # own pinned readback buffers instead of the slot's
+    pack_class: Any = None  # (storage dtype, precision) of a forward request that may be packed
+    group: list | None = None  # [members still running] of the packed launch this job is in
 
 
 class _Slot:
@@ -221,12 +248,14 @@ class ProjectionServer:
     concurrently, each on its own stream; admission also respects
     ``memory_budget_bytes`` (120 GiB by default).  ``graphs=True`` captures the
     launch sequence of each (slot, request class) after its first run and replays it;
-    ``autotune=True`` picks the detector tile per request class.
+    ``autotune=True`` picks the detector tile per request class; ``packing=True`` runs forward
+    requests below ``pack_samples`` nominal ray-samples that wait together as one launch.
     """
 
     def __init__(self, device: str = "cuda:0", *, memory_budget_bytes: int = 120 << 30, slots: int = 4,
                  graphs: bool = True, autotune: bool = True, workspaces_per_slot: int = 64,
-                 graph_samples: int = 1 << 30, exclusive_samples: int = 1 << 30) -> None:
+                 graph_samples: int = 1 << 30, exclusive_samples: int = 1 << 30, packing: bool = True,
+                 pack_samples: int = 1 << 26) -> None:
         import torch
 
         self.torch = torch
@@ -241,6 +270,15 @@ class ProjectionServer:
         self.graph_samples = graph_samples
         self.exclusive_samples = exclusive_samples
         self.large_running = 0
+        self.packing = packing
+        self.pack_samples = pack_samples
+        self.packs = 0  # packed launches made
+        self.packed_requests = 0  # requests that ran inside them
+        # one pack in flight per pack class: packs of one class share its workspaces (packs of
+        # two classes never do: the storage dtype and precision are part of a workspace's key)
+        self.packs_running: set[Any] = set()
+        self.pack_workspaces: OrderedDict[Any, Any] = OrderedDict()
+        self.pack_workspace_limit = 256
         self.autotune = autotune
         self.workspaces_per_slot = workspaces_per_slot
         self.volumes: dict[str, _Volume] = {}
@@ -273,6 +311,8 @@ class ProjectionServer:
     def remove_volume(self, name: str) -> None:
         with self.lock:
             self.volumes.pop(name)
+            for key in [k for k in self.pack_workspaces if k[0] == name]:
+                del self.pack_workspaces[key]
             for slot in self.slots:
                 for key in [k for k in slot.workspaces if k[0] == name]:
                     del slot.workspaces[key]
@@ -291,6 +331,9 @@ class ProjectionServer:
         job.large = self._large(request)
         job.key = (request.volume, batched(request.geometry), request.samples_per_ray, request.precision,
                    request.kind)
+        if self.packing and request.kind == "forward" and not job.large and \
+                batched(request.geometry).pixels * request.samples_per_ray < self.pack_samples:
+            job.pack_class = (str(self.volumes[request.volume].field.dtype), request.precision)
         with self.lock:
             if self.closed:
                 raise ContractError("server is closed")
@@ -396,6 +439,7 @@ class ProjectionServer:
 
                 taken = self.admission.take(len(free), eligible)
                 self.large_running = large_now
+                launches = []
                 for job, _ in taken:
                     # prefer a free slot that already holds this class's workspace and graph
                     slot = next((s for s in free if job.key in s.classes), free[0])
@@ -403,15 +447,35 @@ class ProjectionServer:
                     slot.busy = True
                     slot.classes.add(job.key)
                     job.slot = slot
-            for job, _ in taken:
+                    group = [job]
+                    if job.pack_class is not None and job.pack_class not in self.packs_running:
+                        # small forward requests of one class waiting now join this one's launch
+                        from ._native import MAX_PACK
+
+                        group += [companion for companion, _ in self.admission.take_matching(
+                            lambda other, c=job.pack_class: other.pack_class == c, MAX_PACK - 1)]
+                    if len(group) > 1:
+                        self.packs_running.add(job.pack_class)
+                        running = [len(group)]
+                        for member in group:
+                            member.slot = slot
+                            member.group = running
+                    launches.append(group)
+            for group in launches:
+                started = time.perf_counter()
                 try:
-                    job.started = time.perf_counter()
-                    self._launch(job, use_graph=self.graphs and self._small(job.request))
-                except BaseException as error:  # surfaced through the future
-                    job.outputs["error"] = error
-                    job.event = None
+                    for job in group:
+                        job.started = started
+                    if len(group) > 1:
+                        self._launch_pack(group)
+                    else:
+                        self._launch(group[0], use_graph=self.graphs and self._small(group[0].request))
+                except BaseException as error:  # surfaced through the futures
+                    for job in group:
+                        job.outputs["error"] = error
+                        job.event = None
                 with self.lock:
-                    self.running.append(job)
+                    self.running.extend(group)
                     self.lock.notify_all()
 
     def _startable(self) -> bool:
@@ -441,34 +505,58 @@ class ProjectionServer:
             except BaseException as error:
                 job.future.set_exception(error)
             with self.lock:
-                job.slot.busy = False
+                if job.group is not None:
+                    job.group[0] -= 1  # the slot is free once every member of its pack is done
+                if job.group is None or job.group[0] == 0:
+                    job.slot.busy = False
+                    if job.group is not None:
+                        self.packs_running.discard(job.pack_class)
                 if job.large:
                     self.large_running -= 1
                 self.admission.release(job.nbytes)
                 self.lock.notify_all()
 
     # -------------------------------------------------------- execution
-    def _workspace(self, slot: _Slot, request: ProjectionRequest, block_cols: int):
+    def _workspace_key(self, request: ProjectionRequest, block_cols: int):
+        from .plan import batched
+
+        volume = self.volumes[request.volume]
+        return (request.volume, batched(request.geometry), request.samples_per_ray, request.precision,
+                request.kind, volume.field.dtype, block_cols)
+
+    def _new_workspace(self, request: ProjectionRequest, block_cols: int, pool):
         from .plan import batched, plan_rays
         from .projection import ProjectionSpec, ProjectionWorkspace
 
         volume = self.volumes[request.volume]
-        geometry = batched(request.geometry)
-        key = (request.volume, geometry, request.samples_per_ray, request.precision, request.kind,
-               volume.field.dtype, block_cols)
+        half = volume.field.dtype != self.torch.float32
+        sampling = "compensated" if half else ("float64" if request.precision == "fp64" else "float32")
+        storage = {self.torch.float16: "float16", self.torch.bfloat16: "bfloat16"}.get(volume.field.dtype, "float32")
+        spec = ProjectionSpec(request.samples_per_ray, active_pose=request.kind == "pose",
+                              active_volume=request.kind == "volume",
+                              precision="float64" if request.precision == "fp64" else "float32",
+                              sampling_precision=sampling, storage_precision=storage, block_cols=block_cols)
+        return ProjectionWorkspace(plan_rays(volume.grid, batched(request.geometry)), spec, self.device,
+                                   copies=self.copies, pool=pool)
+
+    def _pack_workspace(self, request: ProjectionRequest, block_cols: int):
+        """The server-wide workspace of a packable request class (forward only: no scratch)."""
+        key = self._workspace_key(request, block_cols)
+        found = self.pack_workspaces.get(key)
+        if found is None:
+            found = self._new_workspace(request, block_cols, None)
+            self.pack_workspaces[key] = found
+            while len(self.pack_workspaces) > self.pack_workspace_limit:
+                self.pack_workspaces.popitem(last=False)
+        else:
+            self.pack_workspaces.move_to_end(key)
+        return found
+
+    def _workspace(self, slot: _Slot, request: ProjectionRequest, block_cols: int):
+        key = self._workspace_key(request, block_cols)
         found = slot.workspaces.get(key)
         if found is None:
-            half = volume.field.dtype != self.torch.float32
-            sampling = "compensated" if half else ("float64" if request.precision == "fp64" else "float32")
-            storage = {self.torch.float16: "float16", self.torch.bfloat16: "bfloat16"}.get(volume.field.dtype,
-                                                                                          "float32")
-            spec = ProjectionSpec(request.samples_per_ray, active_pose=request.kind == "pose",
-                                  active_volume=request.kind == "volume",
-                                  precision="float64" if request.precision == "fp64" else "float32",
-                                  sampling_precision=sampling, storage_precision=storage,
-                                  block_cols=block_cols)
-            found = ProjectionWorkspace(plan_rays(volume.grid, geometry), spec, self.device,
-                                        copies=self.copies, pool=slot.pool)
+            found = self._new_workspace(request, block_cols, slot.pool)
             slot.workspaces[key] = found
             while len(slot.workspaces) > self.workspaces_per_slot:
                 evicted, _ = slot.workspaces.popitem(last=False)
@@ -570,6 +658,40 @@ class ProjectionServer:
             job.workspace = ws
             job.event = torch.cuda.Event()
             job.event.record(slot.stream)
+
+    def _launch_pack(self, jobs: list[_Job]) -> None:
+        """One packed forward launch for ``jobs`` (small forward requests of one class) on
+        their common slot; each job gets its image, status words and the launch's event."""
+        from .projection import forward_packed
+
+        torch = self.torch
+        slot = jobs[0].slot
+        calls, spaces = [], []
+        for job in jobs:
+            request = job.request
+            block_cols = self._block_cols(request, slot)
+            ws = self._pack_workspace(request, block_cols)
+            # poses through a pageable copy: the slot's pinned staging holds one request's only
+            poses = self._poses(request, ws.plan.views)
+            calls.append((ws, self.volumes[request.volume].field, poses))
+            spaces.append(ws)
+        with torch.cuda.stream(slot.stream):
+            images = forward_packed(calls, checked=False)
+            readback = {}
+            for k, ws in enumerate(dict.fromkeys(spaces)):
+                host = slot.pinned(f"status{k}", ws.plan.views, torch.int32)
+                host.copy_(ws.status, non_blocking=True)
+                readback[id(ws)] = host
+            for ws in dict.fromkeys(spaces):
+                ws.status.zero_()
+            event = torch.cuda.Event()
+            event.record(slot.stream)
+        for job, ws, image in zip(jobs, spaces, images, strict=True):
+            job.workspace = ws
+            job.outputs = {"image": image, "status": readback[id(ws)]}
+            job.event = event
+        self.packs += 1
+        self.packed_requests += len(jobs)
 
     def _as_device(self, value):
         torch = self.torch

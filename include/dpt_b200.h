@@ -62,7 +62,7 @@
 extern "C" {
 #endif
 
-#define DPT_B200_ABI_VERSION 3
+#define DPT_B200_ABI_VERSION 4
 
 /* Storage / output element types. */
 enum {
@@ -211,6 +211,18 @@ int dpt_b200_forward(const dpt_problem* problem, const dpt_rays* rays, const voi
 int dpt_b200_vjp(const dpt_problem* problem, const dpt_rays* rays, const void* packed,
                  const void* cotangent, int32_t flags, float* accumulator,
                  double* pose_partials, int32_t* status, void* stream);
+
+/* Forward of several problems in one launch: `count` (<= DPT_MAX_PACK) problems
+ * of one arithmetic, one field layout and one image dtype (else DPT_E_FLAGS), each with its
+ * own rays, field copy (`packed[i]`, as for dpt_b200_forward), image and status words.  One
+ * block runs each (view, tile) item of every problem, so many small requests fill the GPU with
+ * one launch and no tail between them (2^31 - 1 items at most, else a CUDA error); each image
+ * equals its own dpt_b200_forward bit for bit.  No reference counterpart (the reference launches each
+ * view of each call separately); a serving loop's batching of small forward requests. */
+#define DPT_MAX_PACK 64
+int dpt_b200_forward_packed(int32_t count, const dpt_problem* problems, const dpt_rays* rays,
+                            const void* const* packed, void* const* images, int32_t* const* status,
+                            void* stream);
 
 /* Split pose VJP (DPT_ARITH_F32 or DPT_ARITH_F32C, FP32 images).  A ray's pose moments (its
  * sample sum, sums of the grid slopes and of the position-weighted slopes, and for FP32 the

@@ -152,3 +152,26 @@ def test_read_probe_rejects_bad_buffers_without_launching():
     assert lib.dpt_b200_read_probe(16, 0, 1, 16, None) == -2
     assert lib.dpt_b200_read_probe(16, 16, 0, 16, None) == -2
     assert lib.dpt_b200_read_probe(24, 16, 1, 16, None) == -6  # buffer not 16-byte aligned
+
+
+def test_packed_forward_checks_every_descriptor_without_launching():
+    lib = N.library()
+    count = 2
+    problems = (N.Problem * count)(problem(), problem())
+    rays = (N.Rays * count)()
+    for r in rays:
+        r.poses, r.view_table, r.view_count = 16, 16, 1
+    ptrs = lambda *v: (ctypes.c_void_p * count)(*v)  # noqa: E731
+    good = ptrs(16, 16)
+    assert lib.dpt_b200_forward_packed(0, problems, rays, good, good, good, None) == -2
+    assert lib.dpt_b200_forward_packed(N.MAX_PACK + 1, problems, rays, good, good, good, None) == -7
+    assert lib.dpt_b200_forward_packed(count, None, rays, good, good, good, None) == -1
+    assert lib.dpt_b200_forward_packed(count, problems, rays, ptrs(16, None), good, good, None) == -1
+    assert lib.dpt_b200_forward_packed(count, problems, rays, ptrs(16, 24), good, good, None) == -6
+    rays[1].view_begin = 3  # view 3 of a three-view problem
+    assert lib.dpt_b200_forward_packed(count, problems, rays, good, good, good, None) == -5
+    rays[1].view_begin = 0
+    problems[1] = problem(arith=N.ARITH_F64, image_dtype=N.F64)  # a second kernel instantiation
+    assert lib.dpt_b200_forward_packed(count, problems, rays, good, good, good, None) == -4
+    problems[1] = problem(samples=0)
+    assert lib.dpt_b200_forward_packed(count, problems, rays, good, good, good, None) == -2

@@ -215,3 +215,45 @@ def test_admission_holds_back_ineligible_items_without_blocking_the_rest():
     assert [name for name, _ in admission.take(4, eligible)] == ["big1", "small1", "small2"]
     assert [name for name, _ in admission.waiting] == ["big2"]
     assert [name for name, _ in admission.take(4)] == ["big2"]
+
+
+def test_admission_take_matching_fills_a_pack_in_arrival_order_within_the_budget():
+    admission = Admission(100, lookahead=2)
+    for name, size in (("a1", 10), ("b1", 10), ("a2", 70), ("a3", 20), ("b2", 5), ("a4", 30)):
+        admission.offer(name, size)
+    first = admission.take(1)
+    assert [name for name, _ in first] == ["a1"]
+    # the whole queue is scanned (beyond the look-ahead); a2 does not fit beside a3 and a4
+    companions = admission.take_matching(lambda name: name.startswith("a"), limit=8)
+    assert [name for name, _ in companions] == ["a2", "a3"]
+    assert admission.in_use == 100
+    assert [name for name, _ in admission.waiting] == ["b1", "b2", "a4"]
+    admission.release(100)
+    assert [name for name, _ in admission.take_matching(lambda name: True, limit=2)] == ["b1", "b2"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", ["float32", "bfloat16"])
+def test_packed_small_forward_requests_match_each_alone(storage):
+    """A burst of small forward requests on one slot runs as packed launches; every image is
+    the one the same request gives alone, and the gradient requests in the burst are unchanged."""
+    from dpt_b200.serving import ProjectionServer
+
+    scenes, requests = _requests(seed=9, count=24)
+    with ProjectionServer("cuda:0", slots=1, graphs=False, autotune=True) as server:
+        for name, (grid, values) in scenes.items():
+            server.add_volume(name, grid, values, storage=storage)
+        alone = [server.run_alone(request) for request in requests]
+        futures = [server.submit(request) for request in requests + requests]
+        mixed = [future.result(timeout=300) for future in futures]
+        assert server.packs > 0 and server.packed_requests >= 2 * server.packs
+        assert server.admission.in_use == 0
+    for k, request in enumerate(requests + requests):
+        a, m = alone[k % len(requests)], mixed[k]
+        np.testing.assert_array_equal(m.image.cpu().numpy(), a.image.cpu().numpy())
+        if request.kind == "volume":
+            va, vm = a.volume_gradient.float().cpu().numpy(), m.volume_gradient.float().cpu().numpy()
+            assert np.linalg.norm(va - vm) <= 1e-6 * np.linalg.norm(va)
+        if request.kind == "pose":
+            np.testing.assert_allclose(m.pose_gradient.cpu().numpy(), a.pose_gradient.cpu().numpy(),
+                                       rtol=1e-10, atol=1e-13)
