@@ -78,6 +78,10 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--no-graphs", action="store_true", help="serving mode: no CUDA graph replay")
     parser.add_argument("--no-packing", action="store_true",
                         help="serving mode: no packed launches of small forward requests")
+    parser.add_argument("--priority", action="store_true",
+                        help="serving mode: requests that do not fill the GPU on high-priority streams")
+    parser.add_argument("--pack-min", type=int, default=8,
+                        help="serving mode: small forward requests of one class that must wait to form a pack")
     parser.add_argument("--pack-samples", type=int, default=1 << 26,
                         help="serving mode: forward requests below this many nominal ray-samples may be packed")
     return parser.parse_args()
@@ -974,7 +978,7 @@ def run_serving(args) -> None:
 
     with ProjectionServer(str(device), slots=args.slots, autotune=not args.no_autotune,
                           graphs=not args.no_graphs, packing=not args.no_packing,
-                          pack_samples=args.pack_samples) as server:
+                          pack_samples=args.pack_samples, priorities=args.priority, pack_min=args.pack_min) as server:
         for name, (grid, values) in volumes.items():
             for storage in ("float32", "bfloat16"):
                 server.add_volume(f"{name}:{storage}", grid, values, storage=storage)
@@ -1048,7 +1052,8 @@ def run_serving(args) -> None:
                    "latency": "Poisson arrivals at 70% of served capacity, 4 rounds",
                    "slots": args.slots, "memory_budget_gib": 120, "autotune": not args.no_autotune,
                    "graphs": not args.no_graphs, "packing": not args.no_packing,
-                   "pack_samples": args.pack_samples},
+                   "pack_samples": args.pack_samples, "pack_min": args.pack_min,
+                   "priorities": args.priority},
     }
     print(json.dumps(line), flush=True)
 

@@ -96,12 +96,13 @@ def _requests(seed: int = 3, count: int = 14):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("graphs", [False, True])
-def test_results_are_the_same_alone_and_in_the_mix(graphs):
+@pytest.mark.parametrize("graphs,priorities", [(False, False), (True, False), (True, True)])
+def test_results_are_the_same_alone_and_in_the_mix(graphs, priorities):
     from dpt_b200.serving import ProjectionServer
 
     scenes, requests = _requests()
-    with ProjectionServer("cuda:0", slots=4, graphs=graphs, autotune=graphs) as server:
+    with ProjectionServer("cuda:0", slots=4, graphs=graphs, autotune=graphs, priorities=priorities,
+                          exclusive_samples=1 << 18) as server:
         for name, (grid, values) in scenes.items():
             server.add_volume(name, grid, values)
         alone = [server.run_alone(request) for request in requests]
@@ -240,7 +241,7 @@ def test_packed_small_forward_requests_match_each_alone(storage):
     from dpt_b200.serving import ProjectionServer
 
     scenes, requests = _requests(seed=9, count=24)
-    with ProjectionServer("cuda:0", slots=1, graphs=False, autotune=True) as server:
+    with ProjectionServer("cuda:0", slots=1, graphs=False, autotune=True, pack_min=2) as server:
         for name, (grid, values) in scenes.items():
             server.add_volume(name, grid, values, storage=storage)
         alone = [server.run_alone(request) for request in requests]
