@@ -69,7 +69,7 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--seed", type=int, default=20261203)
     parser.add_argument("--mode", choices=("iteration", "serving", "precision", "pointwise", "gather", "panels",
-                                           "table"),
+                                           "table", "packed"),
                         default="iteration",
                         help="iteration: full-scan fwd+VJP step (the headline); serving: mixed request stream")
     parser.add_argument("--requests", type=int, default=48, help="serving mode: requests in the stream")
@@ -1263,6 +1263,62 @@ def run_gather(args) -> None:
         "scatter_vjp_fp64_ms": round(scatter_s * 1e3, 3)}), flush=True)
 
 
+def run_packed(args) -> None:
+    """K forward requests of one shape (FP32 arithmetic, seeded chest phantom, cone views over
+    360 deg with per-request angle offsets): one launch sequence each (``forward``) against one
+    packed launch (``forward_packed``), 20 repetitions after 3 warm ones, CUDA events around
+    the whole batch (host launch cost included: both are enqueued back to back).  Every packed
+    image is first checked equal to its own forward."""
+    import numpy as np
+    import torch
+
+    from dpt_b200.geometry import ConeBeamIntrinsics, RigidTransform
+    from dpt_b200.phantoms import centred_grid, chest_phantom
+    from dpt_b200.plan import plan_rays
+    from dpt_b200.projection import ProjectionSpec, ProjectionWorkspace, forward_packed
+
+    device = "cuda:0"
+    rows = []
+    for shape, detector, views, samples, count in ((64, 128, 1, 128, 32), (128, 128, 2, 256, 32),
+                                                   (128, 256, 4, 256, 16), (256, 512, 8, 512, 8)):
+        grid = centred_grid((shape,) * 3, (1.0, 1.0, 1.0))
+        field = torch.tensor(chest_phantom(grid, seed=args.seed), device=device)
+        pitch = 409.6 / detector
+        pose = torch.tensor(np.tile(RigidTransform().packed(), (views, 1)), dtype=torch.float64, device=device)
+        spaces = []
+        for k in range(count):
+            geometry = ConeBeamIntrinsics(1000.0, 1500.0, (detector, detector), (pitch, pitch)).batch(
+                tuple(2 * math.pi * j / views + 0.01 * k for j in range(views)))
+            spaces.append(ProjectionWorkspace(plan_rays(grid, geometry),
+                                              ProjectionSpec(samples, sampling_precision="float32"), device))
+
+        def each():
+            return [ws.forward(field, pose, checked=False) for ws in spaces]
+
+        def packed():
+            return forward_packed([(ws, field, pose) for ws in spaces], checked=False)
+
+        if not all(torch.equal(a, b) for a, b in zip(each(), packed(), strict=True)):
+            raise SystemExit("packed images differ from the single-request forwards")
+        times = {}
+        for name, run in (("each", each), ("packed", packed)):
+            for _ in range(3):
+                run()
+            torch.cuda.synchronize()
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(20):
+                run()
+            end.record()
+            torch.cuda.synchronize()
+            times[name] = start.elapsed_time(end) / 20
+        rows.append({"requests": count, "grid": shape, "views": views, "detector": detector, "samples": samples,
+                     "one_launch_each_ms": times["each"], "packed_ms": times["packed"],
+                     "speedup": times["each"] / times["packed"]})
+    print(json.dumps({"metric": "packed forward against one launch per request", "unit": "ms per batch",
+                      "arithmetic": "FP32", "rows": rows}), flush=True)
+
+
 def run_panels(args) -> None:
     """Panel kinds and the per-ray pose Jacobian on the full-scan volume: the FP32 forward
     over ``--views`` views of ``--detector``^2 as cone panels, as parallel panels (each
@@ -1495,6 +1551,8 @@ def main() -> None:
         run_panels(args)
     elif args.mode == "table":
         run_table(args)
+    elif args.mode == "packed":
+        run_packed(args)
     else:
         run_gpu(args)
 
