@@ -162,13 +162,18 @@ class Admission:
 class TileTuner:
     """Chooses the detector block tile (8, 16, 32 or 64 columns) per request class.
 
-    ``choose(key, run)`` calls ``run(block_cols)`` -> seconds once per candidate the
-    first time a class is seen and keeps the fastest; later calls return it directly.
+    ``choose(key, run)`` calls ``run(block_cols)`` -> seconds ``repeats`` times per candidate
+    the first time a class is seen and keeps the fastest by its best time; a candidate must
+    beat the default tile (16 columns, the first candidate) by ``margin`` to replace it, so
+    timing noise cannot swap the default for a tile that is no faster.  Later calls return the
+    choice directly.
     """
 
     CANDIDATES = (16, 32, 8, 64)
 
-    def __init__(self) -> None:
+    def __init__(self, repeats: int = 3, margin: float = 0.03) -> None:
+        self.repeats = repeats
+        self.margin = margin
         self.choices: dict[Any, int] = {}
         self.timings: dict[Any, dict[int, float]] = {}
         self.lock = threading.Lock()
@@ -177,8 +182,11 @@ class TileTuner:
         with self.lock:
             if key in self.choices:
                 return self.choices[key]
-        timings = {cols: run(cols) for cols in self.CANDIDATES}
+        timings = {cols: min(run(cols) for _ in range(self.repeats)) for cols in self.CANDIDATES}
+        default = self.CANDIDATES[0]
         best = min(timings, key=timings.get)
+        if timings[best] * (1.0 + self.margin) > timings[default]:
+            best = default
         with self.lock:
             self.timings[key] = timings
             self.choices[key] = best
@@ -756,8 +764,11 @@ class ProjectionServer:
         return self._as_device(request.target).to(ws.spec.image_dtype).reshape(ws.plan.image_shape).clone()
 
     def _body(self, ws, field_tensor, inputs, request: ProjectionRequest) -> dict:
-        """Launch sequence of one request on the current stream (no host synchronisation)."""
-        image = ws.forward(field_tensor, inputs["poses"], checked=False)
+        """Launch sequence of one request on the current stream (no host synchronisation).
+        A pose request in FP32 arithmetic stores its rays' pose moments in the forward, so its
+        pose VJP applies the residual without a second sampling pass."""
+        moments = request.kind == "pose" and ws.moments_preferred()
+        image = ws.forward(field_tensor, inputs["poses"], checked=False, moments=moments)
         out = {"image": image}
         if request.kind != "forward":
             residual = image if inputs["target"] is None else image - inputs["target"]

@@ -39,17 +39,24 @@ def test_admission_respects_slot_count_and_order():
     assert admission.in_use == 50
 
 
-def test_tuner_times_each_candidate_once_and_keeps_the_fastest():
+def test_tuner_keeps_the_fastest_tile_by_its_best_time_and_the_default_within_the_margin():
     calls = []
+    noise = iter([0.0, 0.5, 0.2] * 8)
 
     def run(cols):
         calls.append(cols)
-        return {8: 3.0, 16: 2.0, 32: 1.0, 64: 4.0}[cols]
+        return {8: 3.0, 16: 2.0, 32: 1.0, 64: 4.0}[cols] + next(noise)
 
-    tuner = TileTuner()
+    tuner = TileTuner(repeats=3, margin=0.03)
     assert tuner.choose("k", run) == 32
     assert tuner.choose("k", run) == 32
-    assert sorted(calls) == [8, 16, 32, 64]
+    assert sorted(calls) == sorted([8, 16, 32, 64] * 3)
+    assert tuner.timings["k"] == {8: 3.0, 16: 2.0, 32: 1.0, 64: 4.0}
+
+    # 2 % faster than the default is within the margin: the default stays
+    close = TileTuner(repeats=1, margin=0.03)
+    assert close.choose("c", lambda cols: {8: 3.0, 16: 1.0, 32: 0.98, 64: 4.0}[cols]) == 16
+    assert close.choose("d", lambda cols: {8: 3.0, 16: 1.0, 32: 0.9, 64: 4.0}[cols]) == 32
 
 
 def test_percentiles_and_request_contracts():
