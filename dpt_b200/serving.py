@@ -11,8 +11,8 @@ adds on top of the projector:
   waiting for memory does not block small ones behind it);
 * every admitted request runs on its own CUDA stream, so requests that arrive while
   others are on the GPU overlap on the device; requests that fill the GPU on their own
-  (``exclusive_samples`` nominal ray-samples and more) run one at a time, with smaller ones
-  beside them, because two large requests interleave their blocks and evict each other's
+  (``exclusive_samples`` nominal ray-samples and more) run one at a time, with only small
+  ones (under ``beside_samples``) beside them, because two large requests interleave their blocks and evict each other's
   field copy and accumulator records from L2 (with ``priorities=True`` the smaller ones run
   on high-priority streams, so their blocks start as soon as blocks of the large request
   retire: p50 latency 4.0 against 8.4 ms on a 48-request mix, at 0.66-0.99x the throughput);
@@ -224,6 +224,7 @@ class _Job:
     workspace: Any = None
     key: Any = None  # request class: volume, geometry, samples, precision, kind
     large: bool = False  # fills the GPU on its own: runs while no other large request does
+    medium: bool = False  # not large, but too large to run beside a large request
     private_host: bool = False  # own pinned readback buffers instead of the slot's
     pack_class: Any = None  # (storage dtype, precision) of a forward request that may be packed
     group: list | None = None  # [members still running] of the packed launch this job is in
@@ -280,7 +281,8 @@ class ProjectionServer:
     def __init__(self, device: str = "cuda:0", *, memory_budget_bytes: int = 120 << 30, slots: int = 4,
                  graphs: bool = True, autotune: bool = True, workspaces_per_slot: int = 64,
                  graph_samples: int = 1 << 30, exclusive_samples: int = 1 << 30, packing: bool = True,
-                 pack_samples: int = 1 << 26, pack_min: int = 8, priorities: bool = False) -> None:
+                 pack_samples: int = 1 << 26, pack_min: int = 8, priorities: bool = False,
+                 beside_samples: int = 1 << 28) -> None:
         import torch
 
         self.torch = torch
@@ -294,6 +296,7 @@ class ProjectionServer:
         self.graphs = graphs
         self.graph_samples = graph_samples
         self.exclusive_samples = exclusive_samples
+        self.beside_samples = beside_samples
         self.large_running = 0
         self.packing = packing
         self.pack_samples = pack_samples
@@ -357,6 +360,7 @@ class ProjectionServer:
         job = _Job(request, future, time.perf_counter())
         job.nbytes = self.request_bytes(request)
         job.large = self._large(request)
+        job.medium = not job.large and self._large(request, self.beside_samples)
         job.key = (request.volume, batched(request.geometry), request.samples_per_ray, request.precision,
                    request.kind)
         if self.packing and request.kind == "forward" and not job.large and \
@@ -416,14 +420,16 @@ class ProjectionServer:
         return self.slots + ([self.pack_lane] if self.pack_lane is not None else [])
 
     # ---------------------------------------------------------- sizing
-    def _large(self, request: ProjectionRequest) -> bool:
-        """Whether a request fills the GPU on its own (nominal ray-samples of its passes): such
-        requests run one at a time, because two of them interleave their blocks and evict each
-        other's field copy and accumulator records from L2."""
+    def _large(self, request: ProjectionRequest, threshold: int | None = None) -> bool:
+        """Whether a request fills the GPU on its own (nominal ray-samples of its passes at least
+        ``exclusive_samples``, or ``threshold``): such requests run one at a time, because two
+        of them interleave their blocks and evict each other's field copy and accumulator
+        records from L2."""
         from .plan import batched
 
         passes = 1 if request.kind == "forward" else 2
-        return batched(request.geometry).pixels * request.samples_per_ray * passes >= self.exclusive_samples
+        limit = self.exclusive_samples if threshold is None else threshold
+        return batched(request.geometry).pixels * request.samples_per_ray * passes >= limit
 
     def _small(self, request: ProjectionRequest) -> bool:
         """Whether a request is small enough for graph replay to pay (nominal ray-samples)."""
@@ -484,6 +490,8 @@ class ProjectionServer:
                     nonlocal large_now
                     if self._held(job, counts):
                         return False
+                    if job.medium and large_now:
+                        return False
                     if not job.large:
                         return True
                     if large_now:
@@ -542,7 +550,8 @@ class ProjectionServer:
             return False
         # something a general slot may start, within the admission look-ahead
         window = itertools.islice(self.admission.waiting, self.admission.lookahead)
-        return any(not self._held(job, counts) and not (job.large and self.large_running) for job, _ in window)
+        return any(not self._held(job, counts) and not ((job.large or job.medium) and self.large_running)
+                   for job, _ in window)
 
     def _complete(self) -> None:
         while True:
