@@ -644,7 +644,9 @@ def forward_packed(calls, *, checked: bool = True) -> list[torch.Tensor]:
                                                                     first.spec.image_code):
             raise ContractError("packed calls need one sampling arithmetic, field layout and image dtype")
     with contextlib.ExitStack() as stack, torch.cuda.device(first.device):
-        for ws in dict.fromkeys(spaces):  # each workspace once, in call order
+        # each workspace once, in one global order (by identity), so that two packed calls
+        # naming the same workspaces in different orders cannot each hold what the other waits for
+        for ws in sorted(dict.fromkeys(spaces), key=id):
             stack.enter_context(ws.lock)
         count = len(calls)
         problems = (N.Problem * count)()
