@@ -1,4 +1,4 @@
-"""The packed forward (``dpt_b200_forward_packed``): one persistent launch over the
+"""The packed forward (``dpt_b200_forward_packed``): one launch over the
 (view, tile) blocks of several workspaces of one sampling arithmetic, field layout and image
 dtype.  Every image equals that workspace's own ``forward`` bit for bit (the same per-ray
 code and order of summation) and the oracle's image on the same inputs; mixed scenes (cone,
