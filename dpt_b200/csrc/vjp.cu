@@ -50,6 +50,12 @@
 #ifndef DPT_VJP_MIN_BLOCKS_F32C_JOINT
 #define DPT_VJP_MIN_BLOCKS_F32C_JOINT 8
 #endif
+// The FP32 forward that stores the pose moments: 289.1 ms per full scan at six blocks (80
+// registers, 84 bytes spilled), 289.5 at five (88 registers, none spilled), 316.0 at seven;
+// the occupancy does not matter where the FP32 pipe binds.
+#ifndef DPT_VJP_MIN_BLOCKS_F32_MOMENTS
+#define DPT_VJP_MIN_BLOCKS_F32_MOMENTS 6
+#endif
 #ifndef DPT_VJP_MIN_BLOCKS_F64
 #define DPT_VJP_MIN_BLOCKS_F64 3
 #endif
@@ -137,7 +143,8 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                                   ? (kMoments == kStoreMoments ? DPT_VJP_MIN_BLOCKS_F32C_FORWARD
                                                      : (kVol && kPose)             ? DPT_VJP_MIN_BLOCKS_F32C_JOINT
                                                                                    : DPT_VJP_MIN_BLOCKS_F32C)
-                                                  : kArith == DPT_ARITH_F32 ? DPT_VJP_MIN_BLOCKS_F32
+                                                  : kArith == DPT_ARITH_F32 ? (kMoments == kStoreMoments ? DPT_VJP_MIN_BLOCKS_F32_MOMENTS
+                                                                                                         : DPT_VJP_MIN_BLOCKS_F32)
                                                                             : DPT_VJP_MIN_BLOCKS_F64)
     k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
                                                 int mode, float* __restrict__ acc,
