@@ -738,19 +738,18 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                     const double mx = (double)(dims.nx - 1), my = (double)(dims.ny - 1), mz = (double)(dims.nz - 1);
                     double mean = 0.0, dO[3] = {0.0, 0.0, 0.0}, dD[3] = {0.0, 0.0, 0.0};
                     double sl = 0.0, su = 0.0;
-                    double cs[8];
+                    // a cell run's sums of the FP32-rounded increments, in FP32 as the reference
+                    // adds them (FP32 atomics into the FP32 accumulator)
+                    float cs[8];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) cs[c] = 0.0;
+                    for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                     int pending = -1;
-                    CellCache<Field, kVjpReuse> cache;
+                    // the cell's corners widened to FP64 once per cell (exact)
+                    WideCellCache<Field> cache;
                     auto flush64 = [&]() {
-                        float c32[8];
+                        flush_cell(acc, pending, cs);
 #pragma unroll
-                        for (int c = 0; c < 8; ++c) {
-                            c32[c] = (float)cs[c];
-                            cs[c] = 0.0;
-                        }
-                        flush_cell(acc, pending, c32);
+                        for (int c = 0; c < 8; ++c) cs[c] = 0.0f;
                     };
                     auto point_at = [&](int i, double& position, double* p) {
                         position = fma((double)i + 0.5, step, iv.lower);
@@ -779,9 +778,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                             double value = 0.0, gs[3] = {0.0, 0.0, 0.0};
                             if (in) {
                                 cache.fetch(f, X.lower, Y.lower, Z.lower, cell);
-                                double v[8];
-#pragma unroll
-                                for (int c = 0; c < 8; ++c) v[c] = (double)cache.v[c];
+                                const double* v = cache.v;
                                 value = interpolate64(X.fraction, Y.fraction, Z.fraction, v);
                                 const double sx = (p[0] >= 0.0 && p[0] < mx) ? 1.0 : 0.0;
                                 const double sy = (p[1] >= 0.0 && p[1] < my) ? 1.0 : 0.0;
@@ -813,7 +810,7 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                     contribution = contribution * ((c & 4) ? fz : 1.0 - fz);
                                     const float rounded = (float)contribution;
                                     if (!isfinite(rounded)) bits |= 2;
-                                    cs[c] = cs[c] + (double)rounded;
+                                    cs[c] = cs[c] + rounded;
                                 }
                             } else if (pending >= 0) {
                                 flush64();
