@@ -58,9 +58,13 @@
 #endif
 // Strict FP64: the full-scan joint VJP (launches of two views) measured 86.7 ms per 32 views
 // at three blocks (160 registers), 84.3 at four (128, 68 bytes spilled), 83.2 at five (96,
-// 376 bytes spilled to L1).  The mixed, fast and cell-Gauss forms keep three.
+// 376 bytes spilled to L1).  The cell-Gauss joint VJP: 61.5 ms per 32 views at three blocks,
+// 59.3 at four, 66.0 at five.  The mixed and fast forms keep three.
 #ifndef DPT_VJP_MIN_BLOCKS_F64
 #define DPT_VJP_MIN_BLOCKS_F64 5
+#endif
+#ifndef DPT_VJP_MIN_BLOCKS_CELLS
+#define DPT_VJP_MIN_BLOCKS_CELLS 4
 #endif
 #ifndef DPT_VJP_MIN_BLOCKS_FP64_OTHER
 #define DPT_VJP_MIN_BLOCKS_FP64_OTHER 3
@@ -151,8 +155,9 @@ __global__ void __launch_bounds__(kVjpBlock, kArith == DPT_ARITH_F32C
                                                                                    : DPT_VJP_MIN_BLOCKS_F32C)
                                                   : kArith == DPT_ARITH_F32 ? (kMoments == kStoreMoments ? DPT_VJP_MIN_BLOCKS_F32_MOMENTS
                                                                                                          : DPT_VJP_MIN_BLOCKS_F32)
-                                                  : kArith == DPT_ARITH_F64 ? DPT_VJP_MIN_BLOCKS_F64
-                                                                            : DPT_VJP_MIN_BLOCKS_FP64_OTHER)
+                                                  : kArith == DPT_ARITH_F64   ? DPT_VJP_MIN_BLOCKS_F64
+                                                  : kArith == DPT_ARITH_CELLS ? DPT_VJP_MIN_BLOCKS_CELLS
+                                                                              : DPT_VJP_MIN_BLOCKS_FP64_OTHER)
     k_vjp(RayArgs a, Field f, const Seed* __restrict__ cot,
                                                 int mode, float* __restrict__ acc,
                                                 double* __restrict__ partials, MomentArgs ma)
