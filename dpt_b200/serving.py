@@ -467,12 +467,14 @@ class ProjectionServer:
                 launches = []
                 lane = self.pack_lane
                 if lane is not None and not lane.busy:
-                    # the pack lane: the oldest packable request and every waiting one of its
-                    # class, so small forwards never wait for a general slot
-                    first = next((job for job, _ in self.admission.waiting if job.pack_class is not None), None)
+                    # the pack lane: the oldest request of a pack class with pack_min or more
+                    # waiting, and every waiting one of that class (the condition _startable
+                    # tests, so a free lane never leaves a due pack waiting)
+                    due = self._pack_counts()
+                    first = next((job for job, _ in self.admission.waiting
+                                  if due.get(job.pack_class, 0) >= self.pack_min), None)
                     group = []
-                    if first is not None and sum(job.pack_class == first.pack_class
-                                                 for job, _ in self.admission.waiting) >= self.pack_min:
+                    if first is not None:
                         group = [job for job, _ in self.admission.take_matching(
                             lambda other, c=first.pack_class: other.pack_class == c, MAX_PACK)]
                     if group:
@@ -510,6 +512,10 @@ class ProjectionServer:
                     slot.stream = slot.normal if job.large else slot.urgent
                     job.slot = slot
                     launches.append([job])
+                if not launches:
+                    # nothing fits the memory budget now: wait for a completion to release some
+                    self.lock.wait(0.05)
+                    continue
             for group in launches:
                 started = time.perf_counter()
                 try:
