@@ -159,6 +159,79 @@ class Admission:
             raise ContractError("released more memory than was admitted")
 
 
+class LaunchPolicy:
+    """Which waiting requests start now (no GPU needed).
+
+    Items carry ``pack_class`` (None, or the class of a forward request small enough to pack),
+    ``large`` (fills the GPU on its own) and ``medium`` (too large to run beside a large one).
+    With a pack lane, a pack class is due when ``pack_min`` or more of its items wait; the lane
+    takes the oldest due item's class whole (up to ``max_pack``), and the general slots leave
+    the items of a due class for it.  Large items run one at a time; while one runs, medium
+    items wait too.
+    """
+
+    def __init__(self, pack_min: int, max_pack: int, lane: bool) -> None:
+        self.pack_min = pack_min
+        self.max_pack = max_pack
+        self.lane = lane
+
+    @staticmethod
+    def pack_counts(admission: Admission) -> dict[Any, int]:
+        counts: dict[Any, int] = {}
+        for item, _ in admission.waiting:
+            if item.pack_class is not None:
+                counts[item.pack_class] = counts.get(item.pack_class, 0) + 1
+        return counts
+
+    def held(self, item: Any, counts: dict[Any, int]) -> bool:
+        """Whether a waiting item is kept for the pack lane's next launch."""
+        return self.lane and counts.get(item.pack_class, 0) >= self.pack_min
+
+    def take_pack(self, admission: Admission) -> list[Any]:
+        """The due pack, taken from the queue (empty when none is due or none fits)."""
+        if not self.lane:
+            return []
+        counts = self.pack_counts(admission)
+        first = next((item for item, _ in admission.waiting
+                      if counts.get(item.pack_class, 0) >= self.pack_min), None)
+        if first is None:
+            return []
+        return [item for item, _ in admission.take_matching(
+            lambda other, c=first.pack_class: other.pack_class == c, self.max_pack)]
+
+    def take_singles(self, admission: Admission, free_slots: int, large_running: int) -> tuple[list[Any], int]:
+        """Items for the free general slots, in arrival order, and the new large count."""
+        counts = self.pack_counts(admission)
+        large_now = large_running
+
+        def eligible(item: Any) -> bool:
+            nonlocal large_now
+            if self.held(item, counts) or (item.medium and large_now):
+                return False
+            if not item.large:
+                return True
+            if large_now:
+                return False
+            large_now += 1
+            return True
+
+        taken = [item for item, _ in admission.take(free_slots, eligible)]
+        return taken, large_now
+
+    def startable(self, admission: Admission, lane_free: bool, any_slot_free: bool, large_running: int) -> bool:
+        """Whether a scheduling pass would start something (the scheduler sleeps otherwise)."""
+        if not admission.waiting:
+            return False
+        counts = self.pack_counts(admission)
+        if self.lane and lane_free and counts and max(counts.values()) >= self.pack_min:
+            return True
+        if not any_slot_free:
+            return False
+        window = itertools.islice(admission.waiting, admission.lookahead)
+        return any(not self.held(item, counts) and not ((item.large or item.medium) and large_running)
+                   for item, _ in window)
+
+
 class TileTuner:
     """Chooses the detector block tile (8, 16, 32 or 64 columns) per request class.
 
@@ -308,6 +381,9 @@ class ProjectionServer:
         self.pack_lane = _Slot(torch, self.device, slots, priorities=priorities) if packing else None
         if self.pack_lane is not None:
             self.pack_lane.stream = self.pack_lane.urgent
+        from ._native import MAX_PACK
+
+        self.policy = LaunchPolicy(pack_min, MAX_PACK, self.pack_lane is not None)
         self.pack_workspaces: OrderedDict[Any, Any] = OrderedDict()
         self.pack_workspace_limit = 256
         self.autotune = autotune
@@ -456,8 +532,6 @@ class ProjectionServer:
 
     # ------------------------------------------------------- scheduling
     def _schedule(self) -> None:
-        from ._native import MAX_PACK
-
         while True:
             with self.lock:
                 while not self.closed and not self._startable():
@@ -467,16 +541,7 @@ class ProjectionServer:
                 launches = []
                 lane = self.pack_lane
                 if lane is not None and not lane.busy:
-                    # the pack lane: the oldest request of a pack class with pack_min or more
-                    # waiting, and every waiting one of that class (the condition _startable
-                    # tests, so a free lane never leaves a due pack waiting)
-                    due = self._pack_counts()
-                    first = next((job for job, _ in self.admission.waiting
-                                  if due.get(job.pack_class, 0) >= self.pack_min), None)
-                    group = []
-                    if first is not None:
-                        group = [job for job, _ in self.admission.take_matching(
-                            lambda other, c=first.pack_class: other.pack_class == c, MAX_PACK)]
+                    group = self.policy.take_pack(self.admission)
                     if group:
                         lane.busy = True
                         running = [len(group)]
@@ -485,25 +550,8 @@ class ProjectionServer:
                             member.group = running
                         launches.append(group)
                 free = [slot for slot in self.slots if not slot.busy]
-                large_now = self.large_running
-                counts = self._pack_counts()
-
-                def eligible(job: _Job) -> bool:
-                    nonlocal large_now
-                    if self._held(job, counts):
-                        return False
-                    if job.medium and large_now:
-                        return False
-                    if not job.large:
-                        return True
-                    if large_now:
-                        return False
-                    large_now += 1
-                    return True
-
-                taken = self.admission.take(len(free), eligible)
-                self.large_running = large_now
-                for job, _ in taken:
+                taken, self.large_running = self.policy.take_singles(self.admission, len(free), self.large_running)
+                for job in taken:
                     # prefer a free slot that already holds this class's workspace and graph
                     slot = next((s for s in free if job.key in s.classes), free[0])
                     free.remove(slot)
@@ -533,31 +581,10 @@ class ProjectionServer:
                     self.running.extend(group)
                     self.lock.notify_all()
 
-    def _pack_counts(self) -> dict[Any, int]:
-        """Waiting packable requests per pack class."""
-        counts: dict[Any, int] = {}
-        for job, _ in self.admission.waiting:
-            if job.pack_class is not None:
-                counts[job.pack_class] = counts.get(job.pack_class, 0) + 1
-        return counts
-
-    def _held(self, job: _Job, counts: dict[Any, int]) -> bool:
-        """Whether a waiting request is kept for the pack lane's next launch."""
-        return self.pack_lane is not None and counts.get(job.pack_class, 0) >= self.pack_min
-
     def _startable(self) -> bool:
-        if not self.admission.waiting:
-            return False
-        counts = self._pack_counts()
         lane = self.pack_lane
-        if lane is not None and not lane.busy and counts and max(counts.values()) >= self.pack_min:
-            return True
-        if all(slot.busy for slot in self.slots):
-            return False
-        # something a general slot may start, within the admission look-ahead
-        window = itertools.islice(self.admission.waiting, self.admission.lookahead)
-        return any(not self._held(job, counts) and not ((job.large or job.medium) and self.large_running)
-                   for job, _ in window)
+        return self.policy.startable(self.admission, lane is not None and not lane.busy,
+                                     any(not slot.busy for slot in self.slots), self.large_running)
 
     def _complete(self) -> None:
         while True:

@@ -265,3 +265,59 @@ def test_packed_small_forward_requests_match_each_alone(storage):
         if request.kind == "pose":
             np.testing.assert_allclose(m.pose_gradient.cpu().numpy(), a.pose_gradient.cpu().numpy(),
                                        rtol=1e-10, atol=1e-13)
+
+
+def _items(*specs):
+    """(name, pack_class, large, medium) -> simple request stand-ins."""
+    from types import SimpleNamespace
+
+    return [SimpleNamespace(name=n, pack_class=c, large=lg, medium=md) for n, c, lg, md in specs]
+
+
+def test_launch_policy_packs_the_oldest_due_class_and_holds_it_from_the_slots():
+    from dpt_b200.serving import LaunchPolicy
+
+    admission = Admission(1000)
+    items = _items(("a1", "A", False, False), ("b1", "B", False, False), ("a2", "A", False, False),
+                   ("x", None, False, False), ("b2", "B", False, False), ("b3", "B", False, False))
+    for item in items:
+        admission.offer(item, 10)
+    policy = LaunchPolicy(pack_min=3, max_pack=64, lane=True)
+    # class B is due (3 waiting), A is not: the lane takes all of B, the oldest due class
+    assert policy.startable(admission, lane_free=True, any_slot_free=False, large_running=0)
+    assert [i.name for i in policy.take_pack(admission)] == ["b1", "b2", "b3"]
+    assert policy.take_pack(admission) == []
+    taken, large = policy.take_singles(admission, free_slots=4, large_running=0)
+    assert [i.name for i in taken] == ["a1", "a2", "x"] and large == 0
+
+
+def test_launch_policy_keeps_a_due_class_for_the_busy_lane_and_sleeps_when_nothing_can_start():
+    from dpt_b200.serving import LaunchPolicy
+
+    admission = Admission(1000)
+    for item in _items(("a1", "A", False, False), ("a2", "A", False, False)):
+        admission.offer(item, 10)
+    policy = LaunchPolicy(pack_min=2, max_pack=64, lane=True)
+    # the lane is busy: the slots must not take the due class, so there is nothing to start
+    assert not policy.startable(admission, lane_free=False, any_slot_free=True, large_running=0)
+    assert policy.take_singles(admission, free_slots=4, large_running=0) == ([], 0)
+    # without a lane the same items are ordinary requests
+    plain = LaunchPolicy(pack_min=2, max_pack=64, lane=False)
+    assert plain.startable(admission, lane_free=False, any_slot_free=True, large_running=0)
+    assert plain.take_pack(admission) == []
+    assert [i.name for i in plain.take_singles(admission, 4, 0)[0]] == ["a1", "a2"]
+
+
+def test_launch_policy_runs_large_requests_alone_with_only_small_ones_beside():
+    from dpt_b200.serving import LaunchPolicy
+
+    admission = Admission(1000)
+    for item in _items(("L1", None, True, False), ("m1", None, False, True), ("L2", None, True, False),
+                       ("s1", None, False, False)):
+        admission.offer(item, 10)
+    policy = LaunchPolicy(pack_min=8, max_pack=64, lane=True)
+    taken, large = policy.take_singles(admission, free_slots=4, large_running=0)
+    assert [i.name for i in taken] == ["L1", "s1"] and large == 1  # m1 and L2 wait for L1
+    assert not policy.startable(admission, lane_free=True, any_slot_free=True, large_running=1)
+    taken, large = policy.take_singles(admission, free_slots=4, large_running=0)
+    assert [i.name for i in taken] == ["m1", "L2"] and large == 1  # m1 started before L2 in order
