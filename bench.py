@@ -256,7 +256,7 @@ def cpu_sample_rate(grid, geometry, values, samples: int, threads: int):
     from oracle import oracle as O
 
     views = len(geometry.views)
-    chosen = [k * views // CPU_SAMPLE_VIEWS for k in range(CPU_SAMPLE_VIEWS)]
+    chosen = sorted({k * views // CPU_SAMPLE_VIEWS for k in range(CPU_SAMPLE_VIEWS)})
     pose = np.asarray((1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0, 0, 0, 0))
     realised_total, seconds = 0, 0.0
     for view in chosen:
@@ -667,7 +667,7 @@ def parity_record(args, grid, geometry, values, field, target, tangent, step, id
     adjoint = abs(lhs - rhs) / max(abs(lhs), abs(rhs), 1e-300)
 
     views = len(geometry.views)
-    subset = [k * views // 8 for k in range(8)]
+    subset = sorted({k * views // 8 for k in range(8)})  # 8 evenly spaced views (fewer when fewer exist)
     sub_geometry = BatchedGeometry(tuple(geometry.views[k] for k in subset))
     exact = ProjectionWorkspace(plan_rays(grid, sub_geometry),
                                 ProjectionSpec(args.samples, precision="float64", sampling_precision="float64"),
@@ -757,7 +757,7 @@ def forms_record(args, grid, geometry, values, target, truth, tangent, timer, fp
         torch.cuda.empty_cache()
 
     # errors against strict FP64 on the same stored values (8 views, fixed cotangent)
-    subset = [k * views // 8 for k in range(8)]
+    subset = sorted({k * views // 8 for k in range(8)})  # 8 evenly spaced views (fewer when fewer exist)
     sub_geometry = BatchedGeometry(tuple(geometry.views[k] for k in subset))
     plan = plan_rays(grid, sub_geometry)
     rows, cols = sub_geometry.shape_rows_columns
