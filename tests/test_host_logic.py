@@ -144,3 +144,14 @@ def test_cone_batch_helpers():
     grid = GridSpec((4, 4, 4), (1.0, 1.0, 1.0))
     plan = plan_rays(grid, batch)
     assert plan.rays == 360 * 512 * 512
+
+
+def test_packed_forward_rejects_empty_oversized_and_foreign_calls_before_any_launch():
+    from dpt_b200.projection import forward_packed
+
+    with pytest.raises(ContractError):
+        forward_packed([])
+    with pytest.raises(ContractError):
+        forward_packed([(None, None, None)] * (N.MAX_PACK + 1))
+    with pytest.raises(ContractError):  # not a projection workspace
+        forward_packed([("workspace", torch.zeros(2), torch.zeros(12, dtype=torch.float64))])
