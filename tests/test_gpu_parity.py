@@ -277,10 +277,11 @@ def test_signed_linear_domain_accepts_negative_fields():
 @pytest.mark.parametrize("pose_form", ["matrix", "tangent"])
 @pytest.mark.parametrize("volume", [True, False])
 @pytest.mark.parametrize("sampling,storage", [("float32", "float32"), ("compensated", "bfloat16")])
-def test_split_pose_vjp_from_forward_moments_equals_joint_vjp(pose_form, volume, sampling, storage):
+@pytest.mark.parametrize("shape", [(14, 16, 18), (12, 16, 32)])  # the second: power-of-two nx, ny
+def test_split_pose_vjp_from_forward_moments_equals_joint_vjp(pose_form, volume, sampling, storage, shape):
     """A forward that stores the pose moments writes the same image, and the VJP that then
     forms the pose gradient from them (no second sampling pass) equals the joint VJP."""
-    grid, geometry, values = cone_scene()
+    grid, geometry, values = cone_scene(shape=shape)
     poses = poses_for(len(geometry.views), seed=12)
     dtype = torch.bfloat16 if storage == "bfloat16" else torch.float32
     field, pose = device_inputs(values, poses, dtype)
