@@ -321,3 +321,19 @@ def test_launch_policy_runs_large_requests_alone_with_only_small_ones_beside():
     assert not policy.startable(admission, lane_free=True, any_slot_free=True, large_running=1)
     taken, large = policy.take_singles(admission, free_slots=4, large_running=0)
     assert [i.name for i in taken] == ["m1", "L2"] and large == 1  # m1 started before L2 in order
+
+
+def test_launch_policy_pack_respects_the_memory_budget():
+    from dpt_b200.serving import LaunchPolicy
+
+    admission = Admission(25)
+    for item in _items(("a1", "A", False, False), ("a2", "A", False, False), ("a3", "A", False, False)):
+        admission.offer(item, 10)
+    policy = LaunchPolicy(pack_min=3, max_pack=64, lane=True)
+    # due, but only two of the three fit: the pack takes what fits, the rest waits
+    assert [i.name for i in policy.take_pack(admission)] == ["a1", "a2"]
+    assert admission.in_use == 20 and [i.name for i, _ in admission.waiting] == ["a3"]
+    # one waiting item is no longer a due pack; it may go to a slot once memory is released
+    assert policy.take_singles(admission, free_slots=1, large_running=0) == ([], 0)
+    admission.release(20)
+    assert [i.name for i in policy.take_singles(admission, free_slots=1, large_running=0)[0]] == ["a3"]
