@@ -12,8 +12,9 @@ adds on top of the projector:
 * every admitted request runs on its own CUDA stream, so requests that arrive while
   others are on the GPU overlap on the device; requests that fill the GPU on their own
   (``exclusive_samples`` nominal ray-samples and more) run one at a time, with only small
-  ones (under ``beside_samples``) beside them, because two large requests interleave their blocks and evict each other's
-  field copy and accumulator records from L2 (with ``priorities=True`` the smaller ones run
+  ones (under ``beside_samples``) beside them, because requests that run at once interleave
+  their blocks and evict each other's field copy and accumulator records from L2 (with
+  ``priorities=True`` the smaller ones run
   on high-priority streams, so their blocks start as soon as blocks of the large request
   retire: p50 latency 4.0 against 8.4 ms on a 48-request mix, at 0.66-0.99x the throughput);
 * repeated request shapes below ``graph_samples`` nominal ray-samples replay a captured
@@ -27,15 +28,17 @@ adds on top of the projector:
   to the general slots instead: on a mixed stream a fifth concurrent stream interleaves
   their blocks with a large request's and costs more than their launches (96-request mix:
   157-170 requests/s packing every small forward, 185-187 without);
-* the detector tile of each request class comes from a small autotuner that times the
-  candidate tiles once per class and keeps the fastest.
+* the detector tile of each request class comes from a small autotuner that times each
+  candidate tile three times the first time a class is seen and keeps the default unless
+  another is 3 % faster;
+* which waiting requests start is decided by ``LaunchPolicy`` (no GPU needed, so its rules
+  are tested on the CPU).
 
 Results are exactly those of the same request run alone: the kernels are the same and
 requests share no scratch (each slot owns its workspaces).  Packed launches take their
 workspaces from one server-wide set (one per request class, kept across packs) and run one
-at a time; requests of one class
-packed together share that class's workspace and its status words, so a status bit one of
-them raises is reported to each of them.
+at a time; requests of one class packed together share that class's workspace and its
+status words, so a status bit one of them raises is reported to each of them.
 """
 
 from __future__ import annotations
@@ -345,8 +348,9 @@ class ProjectionServer:
     launch sequence of each (slot, request class) after its first run and replays it;
     ``autotune=True`` picks the detector tile per request class; ``packing=True`` runs forward
     requests below ``pack_samples`` nominal ray-samples as one launch when ``pack_min`` or more
-    of one class wait together;
-    ``priorities=True`` runs requests that do not fill the GPU on high-priority streams (lower
+    of one class wait together; while a request of ``exclusive_samples`` or more runs, only
+    requests under ``beside_samples`` start beside it; ``priorities=True`` runs requests that
+    do not fill the GPU on high-priority streams (lower
     latency for them; on the mixed stream, less throughput: their blocks then interleave with
     the large request's and evict its data from L2).
     """
